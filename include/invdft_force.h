@@ -1,0 +1,228 @@
+/*
+ * invdft_force.h -- C ABI of the B200 force evaluation of invDFT.
+ *
+ * The library replaces, for one GPU, the reference's
+ *   InverseDFTSolverFunction<p,pe,mem>          (include/InverseDFTSolverFunction.h:51-384)
+ *   MultiVectorAdjointLinearSolverProblem<mem>  (include/MultiVectorAdjointLinearSolverProblem.h:15-214)
+ * behind plain pointers and sizes.  All arithmetic on the path is FP64 unless
+ * the context is switched to INVDFT_PRECISION_MIXED.
+ *
+ * Vectors ("multi-vectors") are row-major [n_nodes][B]: node index slowest,
+ * vector index fastest, as the reference's dftfe::linearAlgebra::MultiVector
+ * (MultiVectorAdjointLinearSolverProblem.cpp:638).  Every node of the mesh owns a
+ * row, constrained nodes included, like the deal.II vectors of the reference.
+ *
+ * Entry points that take "d_" pointers expect device memory of the current
+ * CUDA device; all others take host memory.  No entry point aborts: failures
+ * are reported through invdft_status and invdft_last_error().
+ * One context per stream; a context is not thread-safe.
+ */
+#ifndef INVDFT_FORCE_H
+#define INVDFT_FORCE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  INVDFT_OK = 0,
+  INVDFT_MAXITER = 1,    /* an iteration cap was reached (results are returned) */
+  INVDFT_NONFINITE = 2,  /* NaN/Inf in an input or produced on the device */
+  INVDFT_BREAKDOWN = 3,  /* Cholesky/Lanczos breakdown in the eigensolver */
+  INVDFT_OOM = 4,
+  INVDFT_BAD_ARG = 5,
+  INVDFT_CUDA_ERROR = 6,
+  INVDFT_NOT_READY = 7   /* call order violated (e.g. compute_rhs before update_psi) */
+} invdft_status;
+
+typedef enum { INVDFT_PRECISION_FP64 = 0, INVDFT_PRECISION_MIXED = 1 } invdft_precision;
+
+typedef struct invdft_ctx invdft_ctx;
+
+/* Constraint set in closed CSR form: node rows[r] = sum_k weights[k] * x[masters[k]]
+ * for k in [ptr[r], ptr[r+1]); an empty row is a homogeneous Dirichlet node.
+ * (dealii::AffineConstraints after close(); dftUtils::constraintMatrixInfo.) */
+typedef struct {
+  int64_t n_rows;
+  const int64_t *rows;
+  const int64_t *ptr;     /* n_rows + 1 */
+  const int64_t *masters;
+  const double *weights;
+} invdft_constraints;
+
+/* Everything InverseDFTSolverFunction::reinit receives
+ * (InverseDFTSolverFunction.cpp:110-450), for one spin channel at the Gamma point. */
+typedef struct {
+  /* parent (wavefunction) mesh: cubic cells, order-p GLL elements, n1 = p+1 */
+  int32_t p;
+  int64_t n_cells;
+  int64_t n_nodes;
+  const int64_t *cell_nodes;   /* [n_cells][n1^3], lexicographic x fastest */
+  const double *cell_h;        /* [n_cells] edge length */
+  const double *gll_nodes;     /* [n1] on [0,1] */
+  const double *gll_weights;   /* [n1] */
+  const double *gauss_points;  /* [n1] on [0,1] */
+  const double *gauss_weights; /* [n1] */
+  invdft_constraints cons_psi; /* hanging + zero boundary */
+  invdft_constraints cons_adj; /* hanging + rho_target < tol (InverseDFTEngine.cpp:1502-1573) */
+  /* parent quadrature data, [n_cells][n1^3] */
+  const double *jxw;
+  const double *v_base;        /* nuclear + Hartree */
+  const double *v_lda;         /* LDA v_xc of the target (scaled by factor_lda) */
+  const double *rho_target_up; /* spin-up target density */
+  const double *weight;        /* loss weights */
+  /* child (Q1 v_xc) mesh, nested in the parent cells */
+  int64_t n_child_cells;
+  int64_t n_child_nodes;
+  const int64_t *child_cell_nodes; /* [n_child_cells][8] */
+  const double *child_jxw;         /* [n_child_cells][8] */
+  invdft_constraints cons_child;   /* hanging only */
+  const int64_t *child_parent;     /* [n_child_cells], non-decreasing */
+  const double *child_offset;      /* [n_child_cells][3] lower corner in parent ref coords */
+  const double *child_scale;       /* [n_child_cells] child size / parent size */
+  const int64_t *pq_child;         /* [n_cells*n1^3] child cell of each parent quad point */
+  const double *pq_xi;             /* [n_cells*n1^3][3] its coordinates in that child */
+  /* physics */
+  int32_t n_states;
+  double n_electrons;
+  double temperature;
+} invdft_problem_desc;
+
+/* Hot-path knobs (inverseDFTParameters.cpp:369-445 names in comments). */
+typedef struct {
+  int32_t cheb_degree;            /* CHEBYSHEV POLYNOMIAL DEGREE (0: ceil(3 sqrt(upper bound)) in [24,500]) */
+  int32_t max_cheb_passes;        /* MAX CHEBYSHEV PASSES */
+  double cheby_tol;               /* CHEBYSHEV FILTER TOLERANCE */
+  double initial_tol_cheb;        /* INITIAL TOL FOR CHEBYSHEV FILTERING */
+  double adaptive_factor_cheb;    /* ADAPTIVE FACTOR FOR CHEBYSHEV FILTERING */
+  double adjoint_initial_tol;     /* INITIAL TOL FOR ADJOINT PROBLEM */
+  double adaptive_factor_adjoint; /* ADAPTIVE FACTOR FOR ADJOINT */
+  int32_t adjoint_max_iter;       /* MAX ITERATIONS FOR ADJOINT PROBLEM */
+  double degeneracy_tol;          /* TOL FOR DEGENERACY */
+  double frac_occ_tol;            /* TOL FOR FRACTIONAL OCCUPANCY */
+  int32_t additional_states;      /* Solve Additional States During Cheb Filtering */
+  int32_t block_size;             /* CHEBY WFC BLOCK SIZE (0 = all states) */
+  int32_t inter_block_size;       /* BLOCK SIZE OF INTERPOLATE */
+  double factor_lda;              /* FACTOR FOR LDA VXC */
+  int32_t lanczos_steps;          /* steps of the spectrum-bound Lanczos run */
+  int32_t precision;              /* invdft_precision */
+} invdft_params;
+
+typedef struct {
+  int32_t passes;            /* Chebyshev passes of this evaluation */
+  double max_residual;       /* final max residual over the tracked states */
+  double cheb_tol;
+  double adjoint_tol;
+  double loss;               /* sum drho^2 w JxW (InverseDFTSolverFunction.cpp:893-900) */
+  double loss_unweighted;
+  double l1_error;           /* sum |drho| JxW (half of int |rho - rho*|) */
+  double int_rho_veff;
+  double fermi_energy;
+  int32_t minres_iters_max;  /* largest per-column MINRES iteration count */
+  int64_t minres_iters_sum;
+  int32_t n_blocks;
+  int32_t n_hx_calls;        /* Hamiltonian applications issued */
+  int64_t n_hx_columns;      /* sum of their block widths */
+  double ms_eigen, ms_density, ms_adjoint, ms_transfer; /* device time per stage */
+  /* filled when profiling is on: CUDA-event time of the cell-matrix GEMM
+   * launches (the dominant kernel) and their algorithmic bytes and flops */
+  int32_t n_cell_gemm;
+  double ms_cell_gemm;
+  double cell_gemm_bytes;
+  double cell_gemm_flops;
+  int64_t n_launches;        /* kernels this evaluation launched */
+  int32_t degree;            /* Chebyshev filter degree used */
+  double upper_bound;        /* Lanczos upper bound of the spectrum */
+} invdft_force_stats;
+
+/* Defaults of the reference's parameters. */
+void invdft_default_params(invdft_params *params);
+
+/* InverseDFTSolverFunction::reinit (InverseDFTSolverFunction.cpp:110) plus
+ * MultiVectorAdjointLinearSolverProblem::reinit/computeDiagonalA
+ * (MultiVectorAdjointLinearSolverProblem.cpp:476-585): uploads the problem,
+ * builds the gather/scatter maps, mass and stiffness diagonals. */
+invdft_status invdft_force_create(const invdft_problem_desc *desc,
+                                  const invdft_params *params, invdft_ctx **ctx);
+void invdft_force_destroy(invdft_ctx *ctx);
+const char *invdft_last_error(const invdft_ctx *ctx);
+invdft_status invdft_set_params(invdft_ctx *ctx, const invdft_params *params);
+
+/* Record CUDA events around every cell-matrix GEMM launch of the following
+ * evaluations (enable != 0) so that invdft_force_stats reports their device time. */
+invdft_status invdft_set_profiling(invdft_ctx *ctx, int32_t enable);
+
+/* Start subspace of the eigensolver (Lowdin coefficients, host [n_nodes][n_states]).
+ * Without it the first evaluation starts from a fixed hash-generated block. */
+invdft_status invdft_set_subspace(invdft_ctx *ctx, const double *X);
+
+/* InverseDFTSolverFunction::getForceVector (InverseDFTSolverFunction.cpp:657-1311),
+ * one spin.  pot [n_child_nodes] is distributed on entry and its constrained
+ * entries are zeroed on exit (:671-676, :1295-1298); force [n_child_nodes] is
+ * overwritten with its constrained entries zero (:1246); *loss receives L. */
+invdft_status invdft_force_eval(invdft_ctx *ctx, double *pot, double *force,
+                                double *loss, invdft_force_stats *stats);
+
+/* InverseDFTSolverFunction::dotProduct with blockSize 1 (:1693-1705). */
+invdft_status invdft_dot(invdft_ctx *ctx, const double *a, const double *b,
+                         int64_t n, double *out);
+
+/* Results of the last evaluation (host copies). */
+invdft_status invdft_get_eigen(invdft_ctx *ctx, double *eig, double *occ, double *fermi);
+invdft_status invdft_get_psi(invdft_ctx *ctx, double *psi);           /* nodal [n_nodes][N] */
+invdft_status invdft_get_density(invdft_ctx *ctx, double *rho);       /* [n_cells*n1^3] total */
+invdft_status invdft_get_child_quad_products(invdft_ctx *ctx, double *S); /* [n_child_cells*8] */
+
+/* Forward map only: solveEigen (:1315-1477) + computeRhoFromPSI (:748-758). */
+invdft_status invdft_solve_eigen(invdft_ctx *ctx, double *pot, invdft_force_stats *stats);
+
+/* --- building blocks, exposed for the adjoint interface and for tests --- */
+
+/* v_KS = v_base + v_xc(child -> parent quad) + factor_lda v_lda and the cell
+ * Hamiltonians (setVEff + computeCellHamiltonianMatrix, :1367-1388). */
+invdft_status invdft_set_potential(invdft_ctx *ctx, const double *pot);
+
+/* Lowdin HX on device blocks: d_y = M^-1/2 C^T sum_e H_e (C M^-1/2 d_x)_e
+ * (KohnShamDFTBaseOperator::HXWithLowdinOrthonormalisedInput as called at
+ * MultiVectorAdjointLinearSolverProblem.cpp:1353). */
+invdft_status invdft_hx(invdft_ctx *ctx, const double *d_x, double *d_y, int32_t B);
+
+/* MultiVectorAdjointLinearSolverProblem::updateInputPsi (:818-910).
+ * d_psi [n_nodes][B] nodal, occ/eig [B] host, d_u [n_cells*n1^3] = drho * w,
+ * degeneracy in CSR (deg_ptr [B+1], deg_idx), mu = Fermi energy. */
+invdft_status invdft_adjoint_update_psi(invdft_ctx *ctx, const double *d_psi,
+                                        const double *occ, const double *d_u,
+                                        const int32_t *deg_ptr, const int32_t *deg_idx,
+                                        double mu, const double *eig, int32_t B);
+/* computeRhs (:616-812): d_rhs [n_nodes][B]. */
+invdft_status invdft_adjoint_compute_rhs(invdft_ctx *ctx, double *d_rhs);
+/* vmult (:1346-1367): d_Ax = Ht d_x - eps .* d_x; zeroes constrained rows of d_x and d_Ax. */
+invdft_status invdft_adjoint_vmult(invdft_ctx *ctx, double *d_Ax, double *d_x);
+/* precondition_Jacobi / precondition_JacobiSqrt (:588-612); omega is unused as in the reference. */
+invdft_status invdft_adjoint_precondition_jacobi(invdft_ctx *ctx, double *d_dst,
+                                                 const double *d_src, double omega);
+invdft_status invdft_adjoint_precondition_jacobi_sqrt(invdft_ctx *ctx, double *d_dst,
+                                                      const double *d_src, double omega);
+/* distributeX (:1003-1141) on the block solution d_x (in place). */
+invdft_status invdft_adjoint_distribute_x(invdft_ctx *ctx, double *d_x);
+/* Block MINRES of DFT-FE's MultiVectorMinResSolver::solve as called at
+ * InverseDFTSolverFunction.cpp:1106-1112 (zero start, distributeX at the end);
+ * iters [B] receives per-column iteration counts. */
+invdft_status invdft_adjoint_solve(invdft_ctx *ctx, double *d_x, double tol, int32_t max_iter,
+                                   int32_t *iters);
+
+/* L-BFGS driver of BFGSInverseDFTSolver::solve with the CP line search
+ * (BFGSInverseDFTSolver.cpp:467-627).  pot is updated in place; losses
+ * [2*max_iter+1] (may be NULL) receives the loss of each force evaluation
+ * (one per iteration plus one per line-search probe). */
+invdft_status invdft_bfgs_solve(invdft_ctx *ctx, double *pot, int32_t max_iter, double tol,
+                                int32_t line_search_iters, double line_search_tol,
+                                int32_t history, double *losses, int32_t *n_evals);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* INVDFT_FORCE_H */

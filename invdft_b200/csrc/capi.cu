@@ -1,0 +1,266 @@
+// extern "C" entry points of include/invdft_force.h.  Every call is wrapped so
+// that no C++ exception or CUDA error crosses the ABI: failures become an
+// invdft_status and a message retrievable with invdft_last_error().
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "context.h"
+
+struct invdft_ctx {
+  std::unique_ptr<invdft::Context> c;
+  std::string err;
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+template <class F> invdft_status guard(invdft_ctx *ctx, F &&f) {
+  if (!ctx || !ctx->c) return INVDFT_BAD_ARG;
+  try {
+    f(*ctx->c);
+    ctx->err.clear();
+    return INVDFT_OK;
+  } catch (const invdft::StatusError &e) {
+    ctx->err = e.what();
+    return (invdft_status)e.status;
+  } catch (const invdft::CudaError &e) {
+    ctx->err = e.what();
+    return INVDFT_CUDA_ERROR;
+  } catch (const std::bad_alloc &) {
+    ctx->err = "host allocation failed";
+    return INVDFT_OOM;
+  } catch (const std::exception &e) {
+    ctx->err = e.what();
+    return INVDFT_BAD_ARG;
+  }
+}
+}  // namespace
+
+namespace invdft {
+int64_t child_node_count(invdft_ctx *ctx) { return (ctx && ctx->c) ? ctx->c->ncn : -1; }
+// Implemented in bfgs.cpp
+invdft_status bfgs_solve(invdft_ctx *ctx, double *pot, int max_iter, double tol, int ls_iters, double ls_tol,
+                         int history, double *losses, int *n_evals);
+}
+
+extern "C" {
+
+void invdft_default_params(invdft_params *p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->cheb_degree = 50;
+  p->max_cheb_passes = 100;
+  p->cheby_tol = 1e-6;
+  p->initial_tol_cheb = 1e-6;
+  p->adaptive_factor_cheb = 100.0;
+  p->adjoint_initial_tol = 1e-11;
+  p->adaptive_factor_adjoint = 1000.0;
+  p->adjoint_max_iter = 5000;
+  p->degeneracy_tol = 0.002;
+  p->frac_occ_tol = 1e-8;
+  p->additional_states = 0;
+  p->block_size = 0;
+  p->inter_block_size = 10;
+  p->factor_lda = 0.0;
+  p->lanczos_steps = 20;
+  p->precision = INVDFT_PRECISION_FP64;
+}
+
+invdft_status invdft_force_create(const invdft_problem_desc *desc, const invdft_params *params,
+                                  invdft_ctx **ctx) {
+  if (!ctx) return INVDFT_BAD_ARG;
+  *ctx = nullptr;
+  try {
+    auto h = std::make_unique<invdft_ctx>();
+    h->c = std::make_unique<invdft::Context>(desc, params);
+    *ctx = h.release();
+    g_create_error.clear();
+    return INVDFT_OK;
+  } catch (const invdft::StatusError &e) {
+    g_create_error = e.what();
+    return (invdft_status)e.status;
+  } catch (const invdft::CudaError &e) {
+    g_create_error = e.what();
+    return INVDFT_CUDA_ERROR;
+  } catch (const std::bad_alloc &) {
+    g_create_error = "host allocation failed";
+    return INVDFT_OOM;
+  } catch (const std::exception &e) {
+    g_create_error = e.what();
+    return INVDFT_BAD_ARG;
+  }
+}
+
+void invdft_force_destroy(invdft_ctx *ctx) { delete ctx; }
+
+const char *invdft_last_error(const invdft_ctx *ctx) {
+  if (!ctx) return g_create_error.c_str();
+  return ctx->err.c_str();
+}
+
+invdft_status invdft_set_params(invdft_ctx *ctx, const invdft_params *params) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!params) throw invdft::StatusError(INVDFT_BAD_ARG, "null params");
+    c.set_params(params);
+  });
+}
+
+invdft_status invdft_set_profiling(invdft_ctx *ctx, int32_t enable) {
+  return guard(ctx, [&](invdft::Context &c) { c.profile = enable != 0; });
+}
+
+invdft_status invdft_set_subspace(invdft_ctx *ctx, const double *X) {
+  return guard(ctx, [&](invdft::Context &c) { c.set_subspace(X); });
+}
+
+invdft_status invdft_force_eval(invdft_ctx *ctx, double *pot, double *force, double *loss,
+                                invdft_force_stats *stats) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!pot || !force || !loss) throw invdft::StatusError(INVDFT_BAD_ARG, "null argument");
+    c.eval(pot, force, loss, stats);
+  });
+}
+
+invdft_status invdft_dot(invdft_ctx *ctx, const double *a, const double *b, int64_t n, double *out) {
+  return guard(ctx, [&](invdft::Context &) {
+    if (!a || !b || !out || n < 0) throw invdft::StatusError(INVDFT_BAD_ARG, "bad dot arguments");
+    double s = 0.0;
+    for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+    *out = s;
+  });
+}
+
+invdft_status invdft_get_eigen(invdft_ctx *ctx, double *eig, double *occ, double *fermi) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!c.have_eig) throw invdft::StatusError(INVDFT_NOT_READY, "no eigensolve yet");
+    if (eig) std::memcpy(eig, c.eig.data(), sizeof(double) * c.N);
+    if (occ && !c.occ.empty()) std::memcpy(occ, c.occ.data(), sizeof(double) * c.N);
+    if (fermi) *fermi = c.mu;
+  });
+}
+
+invdft_status invdft_get_psi(invdft_ctx *ctx, double *psi) {
+  return guard(ctx, [&](invdft::Context &c) {
+    c.psi.download(psi, (size_t)c.nn * c.N, c.stream);
+    INVDFT_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+invdft_status invdft_get_density(invdft_ctx *ctx, double *rho) {
+  return guard(ctx, [&](invdft::Context &c) {
+    c.rho.download(rho, (size_t)c.nc * c.nq, c.stream);
+    INVDFT_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+invdft_status invdft_get_child_quad_products(invdft_ctx *ctx, double *S) {
+  return guard(ctx, [&](invdft::Context &c) {
+    c.S.download(S, (size_t)c.ncc * 8, c.stream);
+    INVDFT_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+invdft_status invdft_solve_eigen(invdft_ctx *ctx, double *pot, invdft_force_stats *stats) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!pot) throw invdft::StatusError(INVDFT_BAD_ARG, "null potential");
+    c.pot_d.upload(pot, c.ncn, c.stream);
+    c.solve_eigen(c.pot_d.p, stats);
+    double sums[4];
+    c.density_and_loss(sums);
+    if (stats) {
+      stats->loss = sums[0];
+      stats->loss_unweighted = sums[1];
+      stats->l1_error = sums[2];
+      stats->int_rho_veff = sums[3];
+    }
+  });
+}
+
+invdft_status invdft_set_potential(invdft_ctx *ctx, const double *pot) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!pot) throw invdft::StatusError(INVDFT_BAD_ARG, "null potential");
+    c.pot_d.upload(pot, c.ncn, c.stream);
+    c.set_potential_device(c.pot_d.p);
+    INVDFT_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+invdft_status invdft_hx(invdft_ctx *ctx, const double *d_x, double *d_y, int32_t B) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!d_x || !d_y || B < 1 || B > c.N) throw invdft::StatusError(INVDFT_BAD_ARG, "bad hx arguments");
+    c.hx(d_x, d_y, B);
+    INVDFT_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+invdft_status invdft_adjoint_update_psi(invdft_ctx *ctx, const double *d_psi, const double *occ, const double *d_u,
+                                        const int32_t *deg_ptr, const int32_t *deg_idx, double mu,
+                                        const double *eig, int32_t B) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!d_psi || !occ || !d_u || !deg_ptr || !deg_idx || !eig || B < 1)
+      throw invdft::StatusError(INVDFT_BAD_ARG, "bad update_psi arguments");
+    std::vector<std::vector<int>> degen(B);
+    for (int i = 0; i < B; ++i) degen[i].assign(deg_idx + deg_ptr[i], deg_idx + deg_ptr[i + 1]);
+    c.adj_update_psi(d_psi, B, 0, occ, d_u, degen, mu, eig, B);
+    INVDFT_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+invdft_status invdft_adjoint_compute_rhs(invdft_ctx *ctx, double *d_rhs) {
+  return guard(ctx, [&](invdft::Context &c) {
+    c.adj_compute_rhs(d_rhs);
+    INVDFT_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+invdft_status invdft_adjoint_vmult(invdft_ctx *ctx, double *d_Ax, double *d_x) {
+  return guard(ctx, [&](invdft::Context &c) {
+    c.adj_vmult(d_Ax, d_x);
+    INVDFT_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+invdft_status invdft_adjoint_precondition_jacobi(invdft_ctx *ctx, double *d_dst, const double *d_src, double) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!c.psi_ready) throw invdft::StatusError(INVDFT_NOT_READY, "updateInputPsi has not been called");
+    c.adj_precondition(d_dst, d_src, false);
+    INVDFT_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+invdft_status invdft_adjoint_precondition_jacobi_sqrt(invdft_ctx *ctx, double *d_dst, const double *d_src,
+                                                      double) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!c.psi_ready) throw invdft::StatusError(INVDFT_NOT_READY, "updateInputPsi has not been called");
+    c.adj_precondition(d_dst, d_src, true);
+    INVDFT_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+invdft_status invdft_adjoint_distribute_x(invdft_ctx *ctx, double *d_x) {
+  return guard(ctx, [&](invdft::Context &c) {
+    c.adj_distribute_x(d_x);
+    INVDFT_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+invdft_status invdft_adjoint_solve(invdft_ctx *ctx, double *d_x, double tol, int32_t max_iter, int32_t *iters) {
+  return guard(ctx, [&](invdft::Context &c) {
+    std::vector<int> its;
+    c.adj_minres(d_x, tol, max_iter, its);
+    if (iters)
+      for (size_t i = 0; i < its.size(); ++i) iters[i] = its[i];
+  });
+}
+
+invdft_status invdft_bfgs_solve(invdft_ctx *ctx, double *pot, int32_t max_iter, double tol,
+                                int32_t line_search_iters, double line_search_tol, int32_t history,
+                                double *losses, int32_t *n_evals) {
+  if (!ctx || !ctx->c || !pot || max_iter < 0 || history < 1) return INVDFT_BAD_ARG;
+  return invdft::bfgs_solve(ctx, pot, max_iter, tol, line_search_iters, line_search_tol, history, losses,
+                            n_evals);
+}
+
+}  // extern "C"

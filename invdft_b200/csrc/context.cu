@@ -1,0 +1,978 @@
+// Host orchestration of the B200 force evaluation.
+//
+// Context::eval follows InverseDFTSolverFunction::getForceVector
+// (src/InverseDFTSolverFunction.cpp:657-1311); the adj_* members follow
+// MultiVectorAdjointLinearSolverProblem (src/MultiVectorAdjointLinearSolverProblem.cpp).
+// All N_dof-sized work runs in the kernels of kernels.cu on one stream; the
+// host only touches N x N matrices and per-column scalars.
+#include "context.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <set>
+
+#include "linalg.h"
+
+namespace invdft {
+
+namespace {
+
+std::vector<double> lagrange_eval(const std::vector<double> &nodes, double x) {
+  const int n = (int)nodes.size();
+  std::vector<double> out(n, 1.0);
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b < n; ++b)
+      if (b != a) out[a] *= (x - nodes[b]) / (nodes[a] - nodes[b]);
+  return out;
+}
+
+std::vector<double> lagrange_deriv(const std::vector<double> &nodes, double x) {
+  const int n = (int)nodes.size();
+  std::vector<double> out(n, 0.0);
+  for (int a = 0; a < n; ++a)
+    for (int m = 0; m < n; ++m) {
+      if (m == a) continue;
+      double t = 1.0 / (nodes[a] - nodes[m]);
+      for (int b = 0; b < n; ++b)
+        if (b != a && b != m) t *= (x - nodes[b]) / (nodes[a] - nodes[b]);
+      out[a] += t;
+    }
+  return out;
+}
+
+void check(bool ok, const char *msg) {
+  if (!ok) throw StatusError(INVDFT_BAD_ARG, msg);
+}
+
+void upload_cons(Cons &c, const invdft_constraints &h, int64_t nnodes, cudaStream_t s) {
+  check(h.n_rows >= 0 && h.n_rows <= nnodes, "constraint row count out of range");
+  c.n = (int)h.n_rows;
+  c.h_rows.assign(h.rows, h.rows + h.n_rows);
+  std::vector<int> rows(h.n_rows), ptr(h.n_rows + 1);
+  for (int64_t r = 0; r < h.n_rows; ++r) {
+    check(h.rows[r] >= 0 && h.rows[r] < nnodes, "constraint row index out of range");
+    rows[r] = (int)h.rows[r];
+  }
+  for (int64_t r = 0; r <= h.n_rows; ++r) ptr[r] = (int)h.ptr[r];
+  const int64_t nm = h.n_rows ? h.ptr[h.n_rows] : 0;
+  std::vector<int> m(nm);
+  for (int64_t k = 0; k < nm; ++k) {
+    check(h.masters[k] >= 0 && h.masters[k] < nnodes, "constraint master out of range");
+    m[k] = (int)h.masters[k];
+  }
+  c.rows.upload(rows, s);
+  c.ptr.upload(ptr, s);
+  c.masters.upload(m, s);
+  c.w.upload(h.weights, (size_t)nm, s);
+  if (nm == 0) c.masters.ensure(1), c.w.ensure(1);
+  if (h.n_rows == 0) c.rows.ensure(1);
+}
+
+// vector condensation x[m] += w x[s]; x[s] = 0 over a closed constraint set
+void condense(const invdft_constraints &c, std::vector<double> &x) {
+  std::vector<double> sv(c.n_rows);
+  for (int64_t r = 0; r < c.n_rows; ++r) sv[r] = x[c.rows[r]];
+  for (int64_t r = 0; r < c.n_rows; ++r)
+    for (int64_t k = c.ptr[r]; k < c.ptr[r + 1]; ++k) x[c.masters[k]] += c.weights[k] * sv[r];
+  for (int64_t r = 0; r < c.n_rows; ++r) x[c.rows[r]] = 0.0;
+}
+
+// node -> list of (source entry, weight) of sum_e A_e y_e condensed by C^T
+void build_scatter(int64_t nrows, int64_t ncell, int per_cell, const int64_t *cell_nodes,
+                   const invdft_constraints &c, std::vector<int> &ptr, std::vector<int> &src,
+                   std::vector<double> &w) {
+  std::vector<int64_t> crow(nrows, -1);
+  for (int64_t r = 0; r < c.n_rows; ++r) crow[c.rows[r]] = r;
+  std::vector<int64_t> cnt(nrows + 1, 0);
+  const int64_t tot = ncell * per_cell;
+  for (int64_t t = 0; t < tot; ++t) {
+    const int64_t n = cell_nodes[t];
+    const int64_t r = crow[n];
+    if (r < 0) cnt[n + 1]++;
+    else
+      for (int64_t k = c.ptr[r]; k < c.ptr[r + 1]; ++k) cnt[c.masters[k] + 1]++;
+  }
+  for (int64_t n = 0; n < nrows; ++n) cnt[n + 1] += cnt[n];
+  if (cnt[nrows] > INT32_MAX) throw StatusError(INVDFT_BAD_ARG, "scatter map larger than 2^31 entries");
+  ptr.assign(cnt.begin(), cnt.end());
+  src.assign(cnt[nrows], 0);
+  w.assign(cnt[nrows], 0.0);
+  std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+  for (int64_t t = 0; t < tot; ++t) {
+    const int64_t n = cell_nodes[t];
+    const int64_t r = crow[n];
+    if (r < 0) {
+      src[fill[n]] = (int)t;
+      w[fill[n]++] = 1.0;
+    } else {
+      for (int64_t k = c.ptr[r]; k < c.ptr[r + 1]; ++k) {
+        const int64_t m = c.masters[k];
+        src[fill[m]] = (int)t;
+        w[fill[m]++] = c.weights[k];
+      }
+    }
+  }
+}
+
+}  // namespace
+
+Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
+  check(d != nullptr, "null problem descriptor");
+  if (pp) prm = *pp;
+  else invdft_default_params(&prm);
+  set_params(&prm);
+  check(d->p >= 1 && d->p <= 7, "FE order must be in [1, 7]");
+  check(d->n_cells > 0 && d->n_nodes > 0, "empty mesh");
+  check(d->n_nodes < INT32_MAX, "more than 2^31 nodes");
+  check(d->n_states >= 1 && d->n_states <= 64, "n_states must be in [1, 64]");
+  check(d->n_child_cells > 0 && d->n_child_nodes > 0, "empty child mesh");
+  check(d->cell_nodes && d->cell_h && d->gll_nodes && d->gll_weights && d->gauss_points && d->gauss_weights,
+        "missing parent mesh arrays");
+  check(d->jxw && d->v_base && d->rho_target_up && d->weight, "missing quadrature data");
+  check(d->child_cell_nodes && d->child_jxw && d->child_parent && d->child_offset && d->child_scale &&
+            d->pq_child && d->pq_xi,
+        "missing child mesh arrays");
+  INVDFT_CUDA(cudaStreamCreate(&stream));  // ordered with the legacy default stream
+  cudaStream_t s = stream;
+  p = d->p;
+  n1 = p + 1;
+  nd = n1 * n1 * n1;
+  nq = nd;
+  nc = d->n_cells;
+  nn = d->n_nodes;
+  ncc = d->n_child_cells;
+  ncn = d->n_child_nodes;
+  N = d->n_states;
+  n_electrons = d->n_electrons;
+  temperature = d->temperature;
+  kT = C_KB * temperature;
+  check(kT > 0.0, "temperature must be positive");
+  for (int64_t t = 0; t < nc * nd; ++t) check(d->cell_nodes[t] >= 0 && d->cell_nodes[t] < nn, "cell node out of range");
+  for (int64_t t = 0; t < ncc * 8; ++t)
+    check(d->child_cell_nodes[t] >= 0 && d->child_cell_nodes[t] < ncn, "child node out of range");
+  for (int64_t c = 0; c < ncc; ++c) {
+    check(d->child_parent[c] >= 0 && d->child_parent[c] < nc, "child parent out of range");
+    if (c) check(d->child_parent[c] >= d->child_parent[c - 1], "child cells must be sorted by parent");
+  }
+  for (int64_t q = 0; q < nc * nq; ++q) check(d->pq_child[q] >= 0 && d->pq_child[q] < ncc, "pq_child out of range");
+
+  // --- 1D element data and reference stiffness
+  std::vector<double> gl(d->gll_nodes, d->gll_nodes + n1), gw(d->gll_weights, d->gll_weights + n1);
+  std::vector<double> gp(d->gauss_points, d->gauss_points + n1), gq(d->gauss_weights, d->gauss_weights + n1);
+  std::vector<double> ph((size_t)n1 * n1), dph((size_t)n1 * n1);
+  for (int q = 0; q < n1; ++q) {
+    auto v = lagrange_eval(gl, gp[q]);
+    auto dv = lagrange_deriv(gl, gp[q]);
+    for (int a = 0; a < n1; ++a) {
+      ph[(size_t)q * n1 + a] = v[a];
+      dph[(size_t)q * n1 + a] = dv[a];
+    }
+  }
+  std::vector<double> M1((size_t)n1 * n1, 0.0), S1((size_t)n1 * n1, 0.0);
+  for (int a = 0; a < n1; ++a)
+    for (int b = 0; b < n1; ++b)
+      for (int q = 0; q < n1; ++q) {
+        M1[a * n1 + b] += ph[q * n1 + a] * gq[q] * ph[q * n1 + b];
+        S1[a * n1 + b] += dph[q * n1 + a] * gq[q] * dph[q * n1 + b];
+      }
+  std::vector<double> K((size_t)nd * nd);
+  for (int i = 0; i < nd; ++i) {
+    const int a = i % n1, b = (i / n1) % n1, c = i / (n1 * n1);
+    for (int j = 0; j < nd; ++j) {
+      const int ap = j % n1, bp = (j / n1) % n1, cp = j / (n1 * n1);
+      K[(size_t)i * nd + j] = S1[a * n1 + ap] * M1[b * n1 + bp] * M1[c * n1 + cp] +
+                              M1[a * n1 + ap] * S1[b * n1 + bp] * M1[c * n1 + cp] +
+                              M1[a * n1 + ap] * M1[b * n1 + bp] * S1[c * n1 + cp];
+    }
+  }
+  std::vector<double> w3(nd);
+  for (int i = 0; i < nd; ++i) w3[i] = gw[i % n1] * gw[(i / n1) % n1] * gw[i / (n1 * n1)];
+
+  // --- lumped mass and stiffness diagonal, condensed as vectors
+  std::vector<double> m(nn, 0.0), kd(nn, 0.0);
+  for (int64_t e = 0; e < nc; ++e) {
+    const double h = d->cell_h[e];
+    check(h > 0.0, "cell size must be positive");
+    for (int l = 0; l < nd; ++l) {
+      const int64_t n = d->cell_nodes[e * nd + l];
+      m[n] += h * h * h * w3[l];
+      kd[n] += h * K[(size_t)l * nd + l];
+    }
+  }
+  condense(d->cons_psi, m);
+  condense(d->cons_psi, kd);
+  std::vector<double> sm(nn), ism(nn), dA(nn), dSA(nn);
+  for (int64_t n = 0; n < nn; ++n) {
+    sm[n] = std::sqrt(m[n]);
+    ism[n] = m[n] > 0.0 ? 1.0 / std::sqrt(m[n]) : 0.0;
+    const double ik = kd[n] > 0.0 ? 1.0 / kd[n] : 0.0;
+    dA[n] = (1.0 / 0.5) * ik * sm[n] * sm[n];
+    dSA[n] = std::sqrt(1.0 / 0.5) * std::sqrt(ik) * sm[n];
+  }
+
+  // --- maps
+  std::vector<int64_t> crow(nn, -1);
+  for (int64_t r = 0; r < d->cons_psi.n_rows; ++r) crow[d->cons_psi.rows[r]] = r;
+  h_free.assign(nn, 1);
+  for (int64_t r = 0; r < d->cons_psi.n_rows; ++r) h_free[d->cons_psi.rows[r]] = 0;
+  std::vector<int> cn(nc * nd), cm(nc * nd);
+  for (int64_t t = 0; t < nc * nd; ++t) {
+    const int64_t n = d->cell_nodes[t];
+    cn[t] = (int)n;
+    cm[t] = crow[n] < 0 ? (int)n : -(int)(crow[n] + 1);
+  }
+  const int64_t nmast = d->cons_psi.n_rows ? d->cons_psi.ptr[d->cons_psi.n_rows] : 0;
+  std::vector<double> cgw(std::max<int64_t>(nmast, 1), 0.0);
+  for (int64_t k = 0; k < nmast; ++k) cgw[k] = d->cons_psi.weights[k] * ism[d->cons_psi.masters[k]];
+  std::vector<int> sp, ssrc;
+  std::vector<double> sw;
+  build_scatter(nn, nc, nd, d->cell_nodes, d->cons_psi, sp, ssrc, sw);
+
+  phi.upload(ph, s);
+  Kref.upload(K, s);
+  cell_h.upload(d->cell_h, nc, s);
+  jxw.upload(d->jxw, nc * nq, s);
+  v_base.upload(d->v_base, nc * nq, s);
+  if (d->v_lda) v_lda.upload(d->v_lda, nc * nq, s);
+  else { v_lda.alloc(nc * nq); v_lda.zero(s); }
+  rho_t.upload(d->rho_target_up, nc * nq, s);
+  weight.upload(d->weight, nc * nq, s);
+  cell_nodes.upload(cn, s);
+  cell_map.upload(cm, s);
+  upload_cons(cpsi, d->cons_psi, nn, s);
+  upload_cons(cadj, d->cons_adj, nn, s);
+  upload_cons(cchild, d->cons_child, ncn, s);
+  cons_gw.upload(cgw, s);
+  sc_ptr.upload(sp, s);
+  sc_src.upload(ssrc, s);
+  sc_w.upload(sw, s);
+  sqrtM.upload(sm, s);
+  invsqrtM.upload(ism, s);
+  diagA.upload(dA, s);
+  diagSqrtA.upload(dSA, s);
+
+  // --- child mesh
+  std::vector<int> chn(ncc * 8), chp(ncc), pqc(nc * nq);
+  for (int64_t t = 0; t < ncc * 8; ++t) chn[t] = (int)d->child_cell_nodes[t];
+  for (int64_t c = 0; c < ncc; ++c) chp[c] = (int)d->child_parent[c];
+  for (int64_t q = 0; q < nc * nq; ++q) pqc[q] = (int)d->pq_child[q];
+  std::vector<int> csp, cssrc;
+  std::vector<double> csw;
+  build_scatter(ncn, ncc, 8, d->child_cell_nodes, d->cons_child, csp, cssrc, csw);
+  std::vector<int> wp, w0, w1;
+  for (int64_t c = 0; c < ncc;) {
+    int64_t e = d->child_parent[c], c1 = c;
+    while (c1 < ncc && d->child_parent[c1] == e && c1 - c < 64) ++c1;
+    wp.push_back((int)e);
+    w0.push_back((int)c);
+    w1.push_back((int)c1);
+    c = c1;
+  }
+  nwork = (int)wp.size();
+  const double g2h[2] = {0.5 - 0.5 / std::sqrt(3.0), 0.5 + 0.5 / std::sqrt(3.0)};
+  ch_nodes.upload(chn, s);
+  ch_parent.upload(chp, s);
+  pq_child.upload(pqc, s);
+  ch_jxw.upload(d->child_jxw, ncc * 8, s);
+  ch_offset.upload(d->child_offset, ncc * 3, s);
+  ch_scale.upload(d->child_scale, ncc, s);
+  pq_xi.upload(d->pq_xi, nc * nq * 3, s);
+  ch_sc_ptr.upload(csp, s);
+  ch_sc_src.upload(cssrc, s);
+  ch_sc_w.upload(csw, s);
+  work_parent.upload(wp, s);
+  work_c0.upload(w0, s);
+  work_c1.upload(w1, s);
+  gll.upload(gl, s);
+  g2.upload(g2h, 2, s);
+
+  fe.n1 = n1; fe.nd = nd; fe.nq = nq; fe.nc = nc; fe.nnodes = nn;
+  fe.phi = phi.p; fe.cell_h = cell_h.p; fe.cell_nodes = cell_nodes.p; fe.cell_map = cell_map.p;
+  fe.cons_ptr = cpsi.ptr.p; fe.cons_masters = cpsi.masters.p; fe.cons_w = cpsi.w.p; fe.cons_gw = cons_gw.p;
+  fe.cons_rows = cpsi.rows.p; fe.ncons = cpsi.n;
+  fe.sc_ptr = sc_ptr.p; fe.sc_src = sc_src.p; fe.sc_w = sc_w.p;
+  fe.inv_sqrt_mass = invsqrtM.p; fe.sqrt_mass = sqrtM.p;
+  cv.ncc = ncc; cv.nchild_nodes = ncn; cv.cell_nodes = ch_nodes.p; cv.jxw = ch_jxw.p; cv.parent = ch_parent.p;
+  cv.offset = ch_offset.p; cv.scale = ch_scale.p; cv.pq_child = pq_child.p; cv.pq_xi = pq_xi.p;
+  cv.sc_ptr = ch_sc_ptr.p; cv.sc_src = ch_sc_src.p; cv.sc_w = ch_sc_w.p;
+  cv.work_parent = work_parent.p; cv.work_c0 = work_c0.p; cv.work_c1 = work_c1.p; cv.nwork = nwork;
+  cv.gll = gll.p; cv.g2 = g2.p;
+
+  alloc_state();
+  adjoint_tol = prm.adjoint_initial_tol;
+  INVDFT_CUDA(cudaStreamSynchronize(s));
+}
+
+Context::~Context() {
+  for (auto e : ev_pool) cudaEventDestroy(e);
+  if (stream) {
+    cudaStreamSynchronize(stream);
+    cudaStreamDestroy(stream);
+  }
+}
+
+void Context::set_params(const invdft_params *pp) {
+  check(pp->cheb_degree >= 1, "cheb_degree must be >= 1");
+  check(pp->max_cheb_passes >= 1, "max_cheb_passes must be >= 1");
+  check(pp->adjoint_max_iter >= 0, "adjoint_max_iter must be >= 0");
+  check(pp->block_size >= 0, "block_size must be >= 0");
+  check(pp->lanczos_steps >= 2, "lanczos_steps must be >= 2");
+  check(pp->precision == INVDFT_PRECISION_FP64 || pp->precision == INVDFT_PRECISION_MIXED, "bad precision");
+  prm = *pp;
+}
+
+void Context::alloc_state() {
+  const int maxB = N;
+  H.alloc((size_t)nc * nd * nd);
+  X.alloc((size_t)nn * N);
+  Yb.alloc((size_t)nn * N);
+  Zb.alloc((size_t)nn * N);
+  Wb.alloc((size_t)nn * N);
+  Ycell.alloc((size_t)nc * nd * std::max(maxB, 2));
+  vks.alloc(nc * nq);
+  rho.alloc(nc * nq);
+  u.alloc(nc * nq);
+  psi.alloc((size_t)nn * N);
+  S.alloc(ncc * 8);
+  pot_d.alloc(ncn);
+  force_d.alloc(ncn);
+  const size_t part = std::max<size_t>({(size_t)nblocks_red * 64 * 64, (size_t)nc * 4, 1024});
+  partial.alloc(part);
+  small.alloc(64 * 64 * 4);
+  lz_v.alloc(nn);
+  lz_w.alloc(nn);
+  lz_p.alloc(nn);
+  set_subspace(nullptr);
+}
+
+void Context::set_subspace(const double *Xh) {
+  std::vector<double> h((size_t)nn * N);
+  if (Xh) {
+    for (size_t t = 0; t < h.size(); ++t) {
+      check(std::isfinite(Xh[t]), "non-finite entry in the start subspace");
+      h[t] = Xh[t];
+    }
+  } else {
+    for (int64_t i = 0; i < nn; ++i)
+      for (int j = 0; j < N; ++j)
+        h[(size_t)i * N + j] = h_free[i] ? hash_uniform((uint64_t)(i * N + j), 11) : 0.0;
+  }
+  X.upload(h, stream);
+  have_eig = false;
+  INVDFT_CUDA(cudaStreamSynchronize(stream));
+}
+
+// ---------------------------------------------------------------------------
+// Hamiltonian application and the eigensolver
+// ---------------------------------------------------------------------------
+void Context::cell_gemm(const double *d_x, int Bw) {
+  const bool rec = profile && ev_used + 2 <= (int)ev_pool.size();
+  if (rec) INVDFT_CUDA(cudaEventRecord(ev_pool[ev_used], stream));
+  launch_hx_cell_gemm(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
+  if (rec) {
+    INVDFT_CUDA(cudaEventRecord(ev_pool[ev_used + 1], stream));
+    ev_used += 2;
+    // algorithmic traffic: cell matrices once, the block once, the cell results once
+    prof_bytes += 8.0 * ((double)nc * nd * nd + (double)nn * Bw + (double)nc * nd * Bw);
+    prof_flops += 2.0 * (double)nc * nd * nd * Bw;
+  }
+}
+
+void Context::profile_begin() {
+  ev_used = 0;
+  prof_bytes = prof_flops = 0.0;
+  if (profile && ev_pool.empty()) {
+    ev_pool.resize(2 * 8192);
+    for (auto &e : ev_pool) INVDFT_CUDA(cudaEventCreate(&e));
+  }
+}
+
+void Context::profile_end(invdft_force_stats *st) {
+  if (!profile || ev_used == 0) return;
+  INVDFT_CUDA(cudaStreamSynchronize(stream));
+  double ms = 0.0;
+  for (int i = 0; i < ev_used; i += 2) {
+    float t = 0.f;
+    INVDFT_CUDA(cudaEventElapsedTime(&t, ev_pool[i], ev_pool[i + 1]));
+    ms += t;
+  }
+  st->n_cell_gemm = ev_used / 2;
+  st->ms_cell_gemm = ms;
+  st->cell_gemm_bytes = prof_bytes;
+  st->cell_gemm_flops = prof_flops;
+}
+
+void Context::hx(const double *d_x, double *d_y, int Bw) {
+  if (!have_H) throw StatusError(INVDFT_NOT_READY, "no potential set");
+  cell_gemm(d_x, Bw);
+  AsmEpilogue epi;
+  epi.kind = AsmEpilogue::STORE;
+  launch_hx_assemble(fe, Ycell.p, d_y, Bw, epi, 0, stream);
+  n_hx++;
+  n_hx_cols += Bw;
+}
+
+void Context::set_potential_device(double *d_pot) {
+  launch_distribute(cchild.rows.p, cchild.ptr.p, cchild.masters.p, cchild.w.p, cchild.n, d_pot, 1, stream);
+  launch_child_to_parent_quad(cv, d_pot, v_base.p, v_lda.p, prm.factor_lda, vks.p, nc * nq, stream);
+  launch_build_cell_h(fe, vks.p, jxw.p, Kref.p, H.p, stream);
+  have_H = true;
+}
+
+namespace {
+__global__ void lincomb_kernel(double *out, double a, const double *x, double b, const double *y, double c,
+                               const double *z, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v = a * x[i];
+  if (y) v += b * y[i];
+  if (z) v += c * z[i];
+  out[i] = v;
+}
+__global__ void copy_columns_kernel(const double *src, int64_t ld, int col0, double *dst, int64_t n, int B) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n * B) return;
+  dst[i] = src[(i / B) * ld + col0 + i % B];
+}
+void lincomb(double *out, double a, const double *x, double b, const double *y, double c, const double *z,
+             int64_t n, cudaStream_t s) {
+  lincomb_kernel<<<ceil_div(n, 256), 256, 0, s>>>(out, a, x, b, y, c, z, n);
+  INVDFT_LAUNCH_CHECK();
+  count_launch();
+}
+void copy_columns(const double *src, int64_t ld, int col0, double *dst, int64_t n, int B, cudaStream_t s) {
+  copy_columns_kernel<<<ceil_div(n * B, 256), 256, 0, s>>>(src, ld, col0, dst, n, B);
+  INVDFT_LAUNCH_CHECK();
+  count_launch();
+}
+}  // namespace
+
+void Context::lanczos_bounds(double &lo, double &hi) {
+  std::vector<double> v0(nn);
+  double nrm = 0.0;
+  for (int64_t i = 0; i < nn; ++i) {
+    v0[i] = h_free[i] ? hash_uniform((uint64_t)i, 7) : 0.0;
+    nrm += v0[i] * v0[i];
+  }
+  nrm = std::sqrt(nrm);
+  for (auto &x : v0) x /= nrm;
+  lz_v.upload(v0, stream);
+  lz_p.zero(stream);
+  std::vector<double> al, be;
+  double beta = 0.0, hv[2];
+  double *v = lz_v.p, *vp = lz_p.p, *w = lz_w.p;
+  for (int it = 0; it < prm.lanczos_steps; ++it) {
+    hx(v, w, 1);
+    launch_coldot(v, w, nn, 1, partial.p, nblocks_red, small.p, stream);
+    INVDFT_CUDA(cudaMemcpyAsync(hv, small.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    INVDFT_CUDA(cudaStreamSynchronize(stream));
+    const double a = hv[0];
+    lincomb(w, 1.0, w, -a, v, -beta, vp, nn, stream);
+    launch_coldot(w, w, nn, 1, partial.p, nblocks_red, small.p, stream);
+    INVDFT_CUDA(cudaMemcpyAsync(hv, small.p, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    INVDFT_CUDA(cudaStreamSynchronize(stream));
+    beta = std::sqrt(std::max(hv[0], 0.0));
+    al.push_back(a);
+    be.push_back(beta);
+    if (!std::isfinite(a) || !std::isfinite(beta)) throw StatusError(INVDFT_NONFINITE, "non-finite Lanczos step");
+    if (beta == 0.0) break;
+    lincomb(vp, 1.0 / beta, w, 0.0, nullptr, 0.0, nullptr, nn, stream);  // vp <- w / beta
+    std::swap(v, vp);                                                      // v <- new, vp <- old
+  }
+  const int k = (int)al.size();
+  std::vector<double> T((size_t)k * k, 0.0), ev, V;
+  for (int i = 0; i < k; ++i) {
+    T[(size_t)i * k + i] = al[i];
+    if (i + 1 < k) T[(size_t)i * k + i + 1] = T[(size_t)(i + 1) * k + i] = be[i];
+  }
+  jacobi_eigh(k, T, ev, V);
+  lo = ev.front();
+  hi = ev.back() + std::fabs(be.back());
+}
+
+int auto_degree(double upper_bound) {
+  // ceil(3 sqrt(b)) clamped to [24, 500]: keeps the per-pass damping of the
+  // wanted edge roughly constant as the spectrum widens with mesh refinement
+  const double m = std::ceil(3.0 * std::sqrt(std::max(upper_bound, 0.0)));
+  return (int)std::min(500.0, std::max(24.0, m));
+}
+
+void Context::chfsi_pass(double a, double b, double a0, std::vector<double> &res) {
+  const int m = prm.cheb_degree > 0 ? prm.cheb_degree : auto_degree(b);
+  const double e = (b - a) / 2.0, c = (b + a) / 2.0;
+  double sigma = e / (a0 - c);
+  const double sigma1 = sigma, gamma = 2.0 / sigma1;
+  // Chebyshev recurrence on three rotating buffers: P0 = X, P1 = first step
+  double *P0 = X.p, *P1 = Yb.p, *P2 = Zb.p;
+  {
+    cell_gemm(P0, N);
+    AsmEpilogue epi;
+    epi.kind = AsmEpilogue::CHEB;
+    epi.alpha = sigma1 / e;
+    epi.c = c;
+    epi.in = P0;
+    epi.prev = nullptr;
+    launch_hx_assemble(fe, Ycell.p, P1, N, epi, 0, stream);
+    n_hx++;
+    n_hx_cols += N;
+  }
+  for (int k = 2; k <= m; ++k) {
+    const double sigma2 = 1.0 / (gamma - sigma);
+    cell_gemm(P1, N);
+    AsmEpilogue epi;
+    epi.kind = AsmEpilogue::CHEB;
+    epi.alpha = 2.0 * sigma2 / e;
+    epi.c = c;
+    epi.beta = sigma * sigma2;
+    epi.in = P1;
+    epi.prev = P0;
+    launch_hx_assemble(fe, Ycell.p, P2, N, epi, 0, stream);
+    n_hx++;
+    n_hx_cols += N;
+    double *t = P0;
+    P0 = P1;
+    P1 = P2;
+    P2 = t;
+    sigma = sigma2;
+  }
+  double *Yf = P1;                 // filtered block
+  double *T1 = (Yf == Yb.p) ? Zb.p : Yb.p;
+  if (T1 == Yf) T1 = X.p;
+  // S = Yf^T Yf -> Cholesky -> Y = Yf L^-T
+  std::vector<double> Sh((size_t)N * N), L, Tm;
+  launch_gram(Yf, Yf, nn, N, partial.p, nblocks_red, small.p, stream);
+  INVDFT_CUDA(cudaMemcpyAsync(Sh.data(), small.p, sizeof(double) * N * N, cudaMemcpyDeviceToHost, stream));
+  INVDFT_CUDA(cudaStreamSynchronize(stream));
+  for (double vv : Sh)
+    if (!std::isfinite(vv)) throw StatusError(INVDFT_NONFINITE, "non-finite overlap matrix in the eigensolver");
+  if (!cholesky_lower(N, Sh, L)) throw StatusError(INVDFT_BREAKDOWN, "overlap matrix not positive definite");
+  lower_inverse_transpose(N, L, Tm);
+  // Y (orthonormal) in Wb
+  INVDFT_CUDA(cudaMemcpyAsync(small.p, Tm.data(), sizeof(double) * N * N, cudaMemcpyHostToDevice, stream));
+  launch_rotate(Yf, small.p, Wb.p, nn, N, stream);
+  // HY into T1, projected Hamiltonian
+  hx(Wb.p, T1, N);
+  std::vector<double> Hp((size_t)N * N), w, Q;
+  launch_gram(Wb.p, T1, nn, N, partial.p, nblocks_red, small.p, stream);
+  INVDFT_CUDA(cudaMemcpyAsync(Hp.data(), small.p, sizeof(double) * N * N, cudaMemcpyDeviceToHost, stream));
+  INVDFT_CUDA(cudaStreamSynchronize(stream));
+  for (int i = 0; i < N; ++i)
+    for (int j = i + 1; j < N; ++j) {
+      const double v = 0.5 * (Hp[(size_t)i * N + j] + Hp[(size_t)j * N + i]);
+      Hp[(size_t)i * N + j] = Hp[(size_t)j * N + i] = v;
+    }
+  jacobi_eigh(N, Hp, w, Q);
+  INVDFT_CUDA(cudaMemcpyAsync(small.p, Q.data(), sizeof(double) * N * N, cudaMemcpyHostToDevice, stream));
+  INVDFT_CUDA(cudaMemcpyAsync(small.p + 64 * 64, w.data(), sizeof(double) * N, cudaMemcpyHostToDevice, stream));
+  // X = Y Q (into X's storage), residual norms
+  double *Xout = X.p;
+  if (Xout == Wb.p || Xout == T1) throw StatusError(INVDFT_CUDA_ERROR, "buffer aliasing in chfsi_pass");
+  launch_rotate_residual(Wb.p, T1, small.p, small.p + 64 * 64, Xout, nn, N, partial.p, nblocks_red,
+                         small.p + 2 * 64 * 64, stream);
+  std::vector<double> r2(N);
+  INVDFT_CUDA(cudaMemcpyAsync(r2.data(), small.p + 2 * 64 * 64, sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
+  INVDFT_CUDA(cudaStreamSynchronize(stream));
+  res.resize(N);
+  for (int i = 0; i < N; ++i) res[i] = std::sqrt(std::max(r2[i], 0.0));
+  eig = w;
+  have_eig = true;
+}
+
+void Context::solve_eigen(double *d_pot, invdft_force_stats *st) {
+  if (counter > 3) {
+    const double prev = tol_cheb;
+    tol_cheb = std::min(prm.cheby_tol, loss_prev / prm.adaptive_factor_cheb);
+    tol_cheb = std::min(tol_cheb, prev);
+  } else {
+    tol_cheb = std::min(prm.cheby_tol, prm.initial_tol_cheb);
+  }
+  set_potential_device(d_pot);
+  double lo, b;
+  lanczos_bounds(lo, b);
+  int passes = 0;
+  double maxres = 0.0;
+  std::vector<double> res;
+  for (;;) {
+    double a, a0;
+    if (!have_eig) {
+      a0 = lo;
+      a = lo + 0.1 * (b - lo);
+    } else {
+      a0 = eig.front();
+      a = eig.back();
+    }
+    chfsi_pass(a, b, a0, res);
+    mu = fermi_energy(eig, n_electrons, kT);
+    occ.resize(N);
+    int homo = 0;
+    for (int i = 0; i < N; ++i) {
+      occ[i] = partial_occupancy(eig[i], mu, kT);
+      if (eig[i] < mu + 1e-3 && homo < i) homo = i;
+    }
+    maxres = 0.0;
+    for (int i = 0; i < N; ++i)
+      if (occ[i] > prm.frac_occ_tol || i <= homo + prm.additional_states) maxres = std::max(maxres, res[i]);
+    ++passes;
+    if (!(maxres > tol_cheb && passes < prm.max_cheb_passes)) break;
+  }
+  // nodal eigenvectors psi = C M^-1/2 X
+  launch_scale_rows(invsqrtM.p, X.p, psi.p, nn, N, stream);
+  launch_distribute(cpsi.rows.p, cpsi.ptr.p, cpsi.masters.p, cpsi.w.p, cpsi.n, psi.p, N, stream);
+  if (st) {
+    st->degree = prm.cheb_degree > 0 ? prm.cheb_degree : auto_degree(b);
+    st->upper_bound = b;
+    st->passes = passes;
+    st->max_residual = maxres;
+    st->cheb_tol = tol_cheb;
+    st->fermi_energy = mu;
+  }
+}
+
+void Context::density_and_loss(double out4[4]) {
+  DevBuf<double> &occd = small;
+  INVDFT_CUDA(cudaMemcpyAsync(occd.p + 3 * 64 * 64, occ.data(), sizeof(double) * N, cudaMemcpyHostToDevice, stream));
+  launch_density(fe, psi.p, occd.p + 3 * 64 * 64, N, rho_t.p, weight.p, jxw.p, vks.p, rho.p, u.p, partial.p, stream);
+  launch_reduce_partials(partial.p, (int)nc, 4, small.p, stream);
+  INVDFT_CUDA(cudaMemcpyAsync(out4, small.p, sizeof(double) * 4, cudaMemcpyDeviceToHost, stream));
+  INVDFT_CUDA(cudaStreamSynchronize(stream));
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint problem
+// ---------------------------------------------------------------------------
+void Context::ensure_adjoint(int Bw) {
+  if (Bw <= B && a_psi.p) return;
+  B = std::max(Bw, B);
+  const size_t v = (size_t)nn * B;
+  a_psi.alloc(v);
+  a_Q1.alloc((size_t)nc * nq * B);
+  a_Q2.alloc((size_t)nc * nq * B);
+  m_r1.alloc(v); m_r2.alloc(v); m_y.alloc(v); m_v.alloc(v); m_w.alloc(v); m_w2.alloc(v);
+  m_yn.alloc(v); m_b.alloc(v); m_x.alloc(v); m_p.alloc(v);
+  a_ujxw.alloc(nc * nq);
+  a_Mu.alloc((size_t)B * B);
+  a_occ4.alloc(B);
+  a_eig.alloc(B);
+  a_coef.alloc((size_t)B * B);
+  m_scal.alloc(16 * 64);
+  m_flags.alloc(3 * 64);
+  const size_t need = (size_t)nc * (size_t)B * B;
+  if (partial.n < need) partial.alloc(need);
+}
+
+void Context::adj_update_psi(const double *d_psi_in, int64_t ld, int col0, const double *occv,
+                             const double *d_u, const std::vector<std::vector<int>> &degen, double mu_in,
+                             const double *e, int Bw) {
+  check(Bw >= 1 && Bw <= 64, "adjoint block width must be in [1, 64]");
+  ensure_adjoint(Bw);
+  B = Bw;
+  copy_columns(d_psi_in, ld, col0, a_psi.p, nn, Bw, stream);
+  launch_distribute(cpsi.rows.p, cpsi.ptr.p, cpsi.masters.p, cpsi.w.p, cpsi.n, a_psi.p, Bw, stream);
+  h_occ.assign(occv, occv + Bw);
+  h_eig.assign(e, e + Bw);
+  a_mu = mu_in;
+  std::vector<double> o4(Bw);
+  for (int i = 0; i < Bw; ++i) o4[i] = 4.0 * h_occ[i];
+  a_occ4.upload(o4, stream);
+  a_eig.upload(h_eig, stream);
+  pairs.clear();
+  pair_ptr.assign(Bw + 1, 0);
+  pair_j.clear();
+  for (int i = 0; i < Bw; ++i) {
+    for (int j : degen[i]) {
+      check(j >= 0 && j < Bw, "degeneracy index out of range");
+      pairs.push_back(i);
+      pairs.push_back(j);
+      pair_j.push_back(j);
+    }
+    pair_ptr[i + 1] = (int)pair_j.size();
+  }
+  d_pairs.upload(pairs, stream);
+  d_pair_ptr.upload(pair_ptr, stream);
+  d_pair_j.upload(pair_j, stream);
+  if (pairs.empty()) { d_pairs.ensure(2); d_pair_j.ensure(1); }
+  launch_scale_rows(jxw.p, d_u, a_ujxw.p, nc * nq, 1, stream);
+  psi_ready = true;
+}
+
+void Context::adj_mu(const std::vector<double> &occv, std::vector<double> &Mu) {
+  const int np = (int)pairs.size() / 2;
+  launch_interp_to_quad(fe, a_psi.p, a_Q1.p, B, stream);
+  launch_pair_quad_sums(fe, a_Q1.p, a_Q1.p, a_ujxw.p, B, d_pairs.p, np, partial.p, stream);
+  std::vector<double> vals(np);
+  if (np) {
+    launch_reduce_partials(partial.p, (int)nc, np, small.p, stream);
+    INVDFT_CUDA(cudaMemcpyAsync(vals.data(), small.p, sizeof(double) * np, cudaMemcpyDeviceToHost, stream));
+    INVDFT_CUDA(cudaStreamSynchronize(stream));
+  }
+  Mu.assign((size_t)B * B, 0.0);
+  for (int k = 0; k < np; ++k) {
+    const int i = pairs[2 * k], j = pairs[2 * k + 1];
+    Mu[(size_t)i * B + j] += 2.0 * occv[i] * vals[k];
+  }
+}
+
+void Context::adj_compute_rhs(double *d_rhs) {
+  if (!psi_ready) throw StatusError(INVDFT_NOT_READY, "updateInputPsi has not been called");
+  adj_mu(h_occ, h_Mu);
+  a_Mu.upload(h_Mu, stream);
+  launch_r_cell(fe, a_psi.p, a_ujxw.p, Ycell.p, B, stream);
+  AsmEpilogue epi;
+  epi.kind = AsmEpilogue::RHS;
+  epi.occ4 = a_occ4.p;
+  epi.Mu = a_Mu.p;
+  epi.psi = a_psi.p;
+  launch_hx_assemble(fe, Ycell.p, d_rhs, B, epi, 0, stream);
+}
+
+void Context::adj_vmult(double *d_Ax, double *d_x) {
+  if (!psi_ready) throw StatusError(INVDFT_NOT_READY, "updateInputPsi has not been called");
+  cell_gemm(d_x, B);
+  AsmEpilogue epi;
+  epi.kind = AsmEpilogue::VMULT;
+  epi.eps = a_eig.p;
+  epi.in = d_x;
+  launch_hx_assemble(fe, Ycell.p, d_Ax, B, epi, 0, stream);
+  launch_set_zero(cpsi.rows.p, cpsi.n, d_x, B, stream);
+  launch_set_zero(cpsi.rows.p, cpsi.n, d_Ax, B, stream);
+  n_hx++;
+  n_hx_cols += B;
+}
+
+void Context::adj_precondition(double *d_dst, const double *d_src, bool sq) {
+  launch_scale_rows(sq ? diagSqrtA.p : diagA.p, d_src, d_dst, nn, B, stream);
+}
+
+void Context::adj_distribute_x(double *d_x) {
+  if (!psi_ready) throw StatusError(INVDFT_NOT_READY, "updateInputPsi has not been called");
+  launch_scale_rows(invsqrtM.p, d_x, d_x, nn, B, stream);
+  launch_distribute(cpsi.rows.p, cpsi.ptr.p, cpsi.masters.p, cpsi.w.p, cpsi.n, d_x, B, stream);
+  const int np = (int)pairs.size() / 2;
+  std::vector<double> dots(np);
+  if (np) {
+    launch_interp_to_quad(fe, d_x, a_Q2.p, B, stream);
+    launch_interp_to_quad(fe, a_psi.p, a_Q1.p, B, stream);
+    launch_pair_quad_sums(fe, a_Q2.p, a_Q1.p, jxw.p, B, d_pairs.p, np, partial.p, stream);
+    launch_reduce_partials(partial.p, (int)nc, np, small.p, stream);
+    INVDFT_CUDA(cudaMemcpyAsync(dots.data(), small.p, sizeof(double) * np, cudaMemcpyDeviceToHost, stream));
+    INVDFT_CUDA(cudaStreamSynchronize(stream));
+  }
+  std::vector<double> ones(B, 1.0), MuU;
+  adj_mu(ones, MuU);
+  double sum_d = 0.0, eta_rhs = 0.0;
+  for (int i = 0; i < B; ++i) {
+    const double dfi = -partial_occupancy_der(h_eig[i], a_mu, kT);
+    sum_d += dfi;
+    eta_rhs += dfi * MuU[(size_t)i * B + i];
+  }
+  const double eta = std::fabs(eta_rhs) < 1e-16 ? 0.0 : eta_rhs / sum_d;
+  a_eta = eta;
+  std::vector<double> coef(np);
+  for (int k = 0; k < np; ++k) {
+    const int i = pairs[2 * k], j = pairs[2 * k + 1];
+    const double der = partial_occupancy_der(h_eig[i], a_mu, kT);
+    double corr = -der * MuU[(size_t)i * B + j];
+    if (i == j) corr += der * eta;
+    coef[k] = -dots[k] + corr;
+  }
+  if (np) {
+    a_coef.upload(coef, stream);
+    launch_nullspace_update(d_x, a_psi.p, nn, B, d_pair_ptr.p, d_pair_j.p, a_coef.p, stream);
+  }
+}
+
+void Context::adj_minres(double *d_x, double tol, int maxit, std::vector<int> &iters) {
+  if (!psi_ready) throw StatusError(INVDFT_NOT_READY, "updateInputPsi has not been called");
+  const int Bw = B;
+  const size_t v = (size_t)nn * Bw;
+  adj_compute_rhs(m_b.p);
+  INVDFT_CUDA(cudaMemsetAsync(d_x, 0, v * sizeof(double), stream));
+  INVDFT_CUDA(cudaMemsetAsync(m_w.p, 0, v * sizeof(double), stream));
+  INVDFT_CUDA(cudaMemsetAsync(m_w2.p, 0, v * sizeof(double), stream));
+  MinresState st;
+  double *sc = m_scal.p;
+  st.beta = sc + 0 * 64; st.oldb = sc + 1 * 64; st.dbar = sc + 2 * 64; st.epsln = sc + 3 * 64;
+  st.phibar = sc + 4 * 64; st.cs = sc + 5 * 64; st.sn = sc + 6 * 64; st.alfa = sc + 7 * 64;
+  st.beta2 = sc + 8 * 64; st.coef1 = sc + 9 * 64; st.oldeps = sc + 10 * 64; st.delta = sc + 11 * 64;
+  st.denom = sc + 12 * 64; st.phi = sc + 13 * 64;
+  st.active = m_flags.p; st.commit = m_flags.p + 64; st.iters = m_flags.p + 128;
+  st.tol = tol;
+  launch_minres_init(m_b.p, diagA.p, m_r1.p, m_r2.p, m_y.p, nn, Bw, partial.p, nblocks_red, stream);
+  launch_reduce_partials(partial.p, nblocks_red, Bw, st.beta2, stream);
+  launch_minres_init_scalars(st, st.beta2, Bw, stream);
+  std::vector<int> act(Bw);
+  const int check_every = 8;
+  for (int itn = 1; itn <= maxit; ++itn) {
+    if ((itn - 1) % check_every == 0) {
+      INVDFT_CUDA(cudaMemcpyAsync(act.data(), st.active, sizeof(int) * Bw, cudaMemcpyDeviceToHost, stream));
+      INVDFT_CUDA(cudaStreamSynchronize(stream));
+      bool any = false;
+      for (int b = 0; b < Bw; ++b) any |= act[b] != 0;
+      if (!any) break;
+    }
+    launch_minres_v(m_y.p, st, m_v.p, nn, Bw, stream);
+    cell_gemm(m_v.p, Bw);
+    AsmEpilogue epi;
+    epi.kind = AsmEpilogue::MINRES;
+    epi.in = m_v.p;
+    epi.prev = m_r1.p;
+    epi.eps = a_eig.p;
+    epi.minres_coef = st.coef1;
+    epi.dot_partial = partial.p;
+    launch_hx_assemble(fe, Ycell.p, m_yn.p, Bw, epi, nblocks_red, stream);
+    launch_reduce_partials(partial.p, nblocks_red, Bw, st.alfa, stream);
+    n_hx++;
+    n_hx_cols += Bw;
+    launch_minres_update1(m_r1.p, m_r2.p, m_y.p, m_yn.p, diagA.p, st, nn, Bw, partial.p, nblocks_red, stream);
+    launch_minres_scalars(st, Bw, itn, stream);
+    launch_minres_update2(d_x, m_w.p, m_w2.p, m_v.p, st, nn, Bw, stream);
+  }
+  iters.assign(Bw, 0);
+  INVDFT_CUDA(cudaMemcpyAsync(iters.data(), st.iters, sizeof(int) * Bw, cudaMemcpyDeviceToHost, stream));
+  INVDFT_CUDA(cudaStreamSynchronize(stream));
+  last_iters = iters;
+  adj_distribute_x(d_x);
+}
+
+void Context::accumulate_child_products(const double *d_psi, const double *d_p, int Bw) {
+  launch_psi_adjoint_child(fe, cv, d_psi, d_p, Bw, S.p, stream);
+}
+
+// ---------------------------------------------------------------------------
+// getForceVector
+// ---------------------------------------------------------------------------
+namespace {
+std::vector<std::vector<int>> degeneracy_map(const std::vector<double> &ev, double tol) {
+  // InverseDFTSolverFunction.cpp:37-77
+  const int n = (int)ev.size();
+  std::map<int, std::set<int>> groups;
+  std::map<int, int> group_of;
+  int count = 0;
+  for (int i = 0; i < n; ++i) {
+    auto it = group_of.find(i);
+    if (it != group_of.end()) {
+      const int g = it->second;
+      for (int j = 0; j < n; ++j)
+        if (std::fabs(ev[i] - ev[j]) < tol) { groups[g].insert(j); group_of[j] = g; }
+    } else {
+      groups[count].insert(i);
+      group_of[i] = count;
+      for (int j = 0; j < n; ++j)
+        if (std::fabs(ev[i] - ev[j]) < tol) { groups[count].insert(j); group_of[j] = count; }
+      ++count;
+    }
+  }
+  std::vector<std::vector<int>> out(n);
+  for (int i = 0; i < n; ++i) {
+    const auto &s = groups[group_of[i]];
+    out[i].assign(s.begin(), s.end());
+  }
+  return out;
+}
+
+struct StageTimer {
+  cudaEvent_t a, b;
+  cudaStream_t s;
+  explicit StageTimer(cudaStream_t st) : s(st) {
+    INVDFT_CUDA(cudaEventCreate(&a));
+    INVDFT_CUDA(cudaEventCreate(&b));
+    INVDFT_CUDA(cudaEventRecord(a, s));
+  }
+  double stop() {
+    INVDFT_CUDA(cudaEventRecord(b, s));
+    INVDFT_CUDA(cudaEventSynchronize(b));
+    float ms = 0.f;
+    INVDFT_CUDA(cudaEventElapsedTime(&ms, a, b));
+    return ms;
+  }
+  ~StageTimer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+};
+}  // namespace
+
+void Context::eval(double *pot, double *force, double *loss, invdft_force_stats *st) {
+  invdft_force_stats local{};
+  if (!st) st = &local;
+  std::memset(st, 0, sizeof(*st));
+  n_hx = 0;
+  n_hx_cols = 0;
+  const long long launches0 = launch_count();
+  profile_begin();
+  for (int64_t i = 0; i < ncn; ++i)
+    if (!std::isfinite(pot[i])) throw StatusError(INVDFT_NONFINITE, "non-finite entry in the potential");
+  pot_d.upload(pot, ncn, stream);
+  StageTimer t_eig(stream);
+  solve_eigen(pot_d.p, st);
+  st->ms_eigen = t_eig.stop();
+  StageTimer t_den(stream);
+  double sums[4];
+  density_and_loss(sums);
+  st->ms_density = t_den.stop();
+  st->loss = sums[0];
+  st->loss_unweighted = sums[1];
+  st->l1_error = sums[2];
+  st->int_rho_veff = sums[3];
+  if (!std::isfinite(sums[0])) throw StatusError(INVDFT_NONFINITE, "non-finite loss");
+  S.zero(stream);
+  StageTimer t_adj(stream);
+  double t_transfer = 0.0;
+  const int block = prm.block_size > 0 ? prm.block_size : N;
+  int jvec = 0, nblk = 0, itmax = 0;
+  int64_t itsum = 0;
+  while (jvec < N) {
+    int bs = std::min(block, N - jvec);
+    for (;;) {
+      const int last = jvec + bs - 1;
+      if (last + 1 != N && std::fabs(eig[last] - eig[last + 1]) < prm.degeneracy_tol) --bs;
+      else break;
+    }
+    if (bs < 1) throw StatusError(INVDFT_BAD_ARG, "degenerate group wider than the block size");
+    std::vector<double> shifts(eig.begin() + jvec, eig.begin() + jvec + bs);
+    std::vector<double> focc(occ.begin() + jvec, occ.begin() + jvec + bs);
+    auto degen = degeneracy_map(shifts, prm.degeneracy_tol);
+    adj_update_psi(psi.p, N, jvec, focc.data(), u.p, degen, mu, shifts.data(), bs);
+    adjoint_tol = std::min(adjoint_tol, tol_cheb / prm.adaptive_factor_adjoint);
+    std::vector<int> its;
+    adj_minres(m_x.p, adjoint_tol, prm.adjoint_max_iter, its);
+    for (int i : its) {
+      itmax = std::max(itmax, i);
+      itsum += i;
+    }
+    INVDFT_CUDA(cudaMemcpyAsync(m_p.p, m_x.p, sizeof(double) * nn * bs, cudaMemcpyDeviceToDevice, stream));
+    launch_distribute(cadj.rows.p, cadj.ptr.p, cadj.masters.p, cadj.w.p, cadj.n, m_p.p, bs, stream);
+    StageTimer t_tr(stream);
+    accumulate_child_products(a_psi.p, m_p.p, bs);
+    t_transfer += t_tr.stop();
+    jvec += bs;
+    ++nblk;
+  }
+  StageTimer t_f(stream);
+  launch_force_project(cv, S.p, force_d.p, stream);
+  force_d.download(force, ncn, stream);
+  INVDFT_CUDA(cudaStreamSynchronize(stream));
+  t_transfer += t_f.stop();
+  st->ms_adjoint = t_adj.stop() - t_transfer;
+  st->ms_transfer = t_transfer;
+  // zero constrained entries of force (hanging, :1246) and pot (:1295-1298)
+  for (int64_t r : cchild.h_rows) {
+    force[r] = 0.0;
+    pot[r] = 0.0;
+  }
+  *loss = sums[0];
+  st->adjoint_tol = adjoint_tol;
+  st->minres_iters_max = itmax;
+  st->minres_iters_sum = itsum;
+  st->n_blocks = nblk;
+  st->n_hx_calls = n_hx;
+  st->n_hx_columns = n_hx_cols;
+  loss_prev = sums[0];
+  ++counter;
+  st->n_launches = launch_count() - launches0;
+  profile_end(st);
+}
+
+}  // namespace invdft

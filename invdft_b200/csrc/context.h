@@ -1,0 +1,123 @@
+// Context of the B200 force evaluation: device-resident problem, state and
+// the host orchestration mirroring InverseDFTSolverFunction and
+// MultiVectorAdjointLinearSolverProblem.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../include/invdft_force.h"
+#include "kernels.cuh"
+
+namespace invdft {
+
+constexpr double C_KB = 3.166811429e-06;  // Ha/K
+int auto_degree(double upper_bound);
+
+struct Cons {                      // device copy of a closed constraint set
+  int n = 0;
+  DevBuf<int> rows, ptr, masters;
+  DevBuf<double> w;
+  std::vector<int64_t> h_rows;     // host copy of the constrained rows
+};
+
+struct Timer {
+  cudaEvent_t a = nullptr, b = nullptr;
+};
+
+class Context {
+ public:
+  Context(const invdft_problem_desc *d, const invdft_params *p);
+  ~Context();
+
+  invdft_params prm;
+  std::string last_error;
+  cudaStream_t stream = nullptr;
+
+  // sizes
+  int p = 0, n1 = 0, nd = 0, nq = 0, N = 0;
+  int64_t nc = 0, nn = 0, ncc = 0, ncn = 0;
+  double n_electrons = 0, temperature = 0, kT = 0;
+
+  // parent data
+  DevBuf<double> phi, Kref, cell_h, jxw, v_base, v_lda, rho_t, weight;
+  DevBuf<int> cell_nodes, cell_map;
+  Cons cpsi, cadj, cchild;
+  DevBuf<double> cons_gw;
+  DevBuf<int> sc_ptr, sc_src;
+  DevBuf<double> sc_w;
+  DevBuf<double> sqrtM, invsqrtM, diagA, diagSqrtA;
+  std::vector<char> h_free;        // unconstrained psi rows
+  // child data
+  DevBuf<int> ch_nodes, ch_parent, pq_child, ch_sc_ptr, ch_sc_src, work_parent, work_c0, work_c1;
+  DevBuf<double> ch_jxw, ch_offset, ch_scale, pq_xi, ch_sc_w, gll, g2;
+  int nwork = 0;
+  FeView fe{};
+  ChildView cv{};
+
+  // eigensolver state
+  DevBuf<double> H;                // [nc][nd][nd] column-major cells
+  DevBuf<double> X, Yb, Zb, Wb;    // [nn][N]
+  DevBuf<double> Ycell;            // [nc][nd][maxB]
+  DevBuf<double> vks, rho, u, psi, S, pot_d, force_d;
+  DevBuf<double> partial, small, lz_v, lz_w, lz_p;
+  std::vector<double> eig, occ;
+  double mu = 0.0;
+  bool have_eig = false;
+  bool have_H = false;
+  int counter = 0;
+  double tol_cheb = 1e-8, loss_prev = 0.0, adjoint_tol = 0.0;
+  int nblocks_red = 1184;
+  // statistics of the current evaluation
+  int n_hx = 0;
+  int64_t n_hx_cols = 0;
+  // optional per-launch timing of the cell GEMM
+  bool profile = false;
+  std::vector<cudaEvent_t> ev_pool;
+  int ev_used = 0;
+  double prof_bytes = 0.0, prof_flops = 0.0;
+  void cell_gemm(const double *d_x, int Bw);
+  void profile_begin();
+  void profile_end(invdft_force_stats *st);
+
+  // adjoint problem state (MultiVectorAdjointLinearSolverProblem)
+  int B = 0;
+  bool psi_ready = false;
+  DevBuf<double> a_psi, a_ujxw, a_Mu, a_occ4, a_eig, a_coef, a_Q1, a_Q2;
+  std::vector<double> h_occ, h_eig, h_Mu;
+  double a_mu = 0.0, a_eta = 0.0;
+  std::vector<int> pairs, pair_ptr, pair_j;
+  DevBuf<int> d_pairs, d_pair_ptr, d_pair_j;
+  // MINRES buffers
+  DevBuf<double> m_r1, m_r2, m_y, m_v, m_w, m_w2, m_yn, m_b, m_x, m_p;
+  DevBuf<double> m_scal;           // 16 * maxB doubles
+  DevBuf<int> m_flags;             // 3 * maxB ints
+  std::vector<int> last_iters;
+
+  // ---- operations ----
+  void set_params(const invdft_params *p);
+  void set_subspace(const double *Xh);
+  void hx(const double *d_x, double *d_y, int Bw);
+  void set_potential_device(double *d_pot);   // distributes d_pot in place
+  void lanczos_bounds(double &lo, double &hi);
+  void chfsi_pass(double a, double b, double a0, std::vector<double> &res);
+  void solve_eigen(double *d_pot, invdft_force_stats *st);
+  void density_and_loss(double out4[4]);
+  // adjoint
+  void adj_update_psi(const double *d_psi_in, int64_t ld, int col0, const double *occ, const double *d_u,
+                      const std::vector<std::vector<int>> &degen, double mu, const double *e, int Bw);
+  void adj_mu(const std::vector<double> &occv, std::vector<double> &Mu_out);
+  void adj_compute_rhs(double *d_rhs);
+  void adj_vmult(double *d_Ax, double *d_x);
+  void adj_precondition(double *d_dst, const double *d_src, bool sqrt_version);
+  void adj_distribute_x(double *d_x);
+  void adj_minres(double *d_x, double tol, int maxit, std::vector<int> &iters);
+  // full evaluation
+  void eval(double *pot, double *force, double *loss, invdft_force_stats *st);
+  void accumulate_child_products(const double *d_psi, const double *d_p, int Bw);
+
+ private:
+  void alloc_state();
+  void ensure_adjoint(int Bw);
+};
+
+}  // namespace invdft

@@ -1,0 +1,1022 @@
+// Device kernels of the invDFT force evaluation, FP64 path, sm_100a.
+//
+// Layout conventions: multi-vectors are [node][B] (B fastest); cell blocks are
+// [cell][local node][B]; quadrature blocks are [cell][q][B]; cell matrices are
+// stored column-major per cell, H[e][j][i], so that thread i of a CTA streams
+// column j of H_e with unit stride.
+#include "kernels.cuh"
+
+#include <atomic>
+
+namespace invdft {
+
+namespace {
+constexpr int NT = 256;
+
+__device__ __forceinline__ double mat1d(const double *A, bool trans, int n1, int q, int a) {
+  return trans ? A[a * n1 + q] : A[q * n1 + a];
+}
+
+// Three-pass tensor-product contraction on a [n1^3][CH] block held in shared
+// memory: out = (A (x) A (x) A) in, or with A^T when trans.  Result lands in t1.
+__device__ void tensor3(const double *A, bool trans, const double *in, double *t1, double *t2,
+                        int n1, int CH) {
+  const int n2 = n1 * n1, n3 = n2 * n1, tot = n3 * CH;
+  for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+    const int k = idx % CH, pt = idx / CH, q = pt % n1, bc = pt / n1;
+    double s = 0.0;
+    for (int a = 0; a < n1; ++a) s = fma(mat1d(A, trans, n1, q, a), in[(a + n1 * bc) * CH + k], s);
+    t1[idx] = s;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+    const int k = idx % CH, pt = idx / CH, q1 = pt % n1, q2 = (pt / n1) % n1, c = pt / n2;
+    double s = 0.0;
+    for (int b = 0; b < n1; ++b) s = fma(mat1d(A, trans, n1, q2, b), t1[(q1 + n1 * b + n2 * c) * CH + k], s);
+    t2[idx] = s;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < tot; idx += blockDim.x) {
+    const int k = idx % CH, pt = idx / CH, q12 = pt % n2, q3 = pt / n2;
+    double s = 0.0;
+    for (int c = 0; c < n1; ++c) s = fma(mat1d(A, trans, n1, q3, c), t2[(q12 + n2 * c) * CH + k], s);
+    t1[idx] = s;
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Cell Hamiltonian H_e = 1/2 h K_ref + N^T diag(v JxW) N by sum factorisation.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) build_cell_h_kernel(int n1, const double *__restrict__ phi,
+                                                          const double *__restrict__ vks,
+                                                          const double *__restrict__ jxw,
+                                                          const double *__restrict__ Kref,
+                                                          const double *__restrict__ cell_h,
+                                                          double *__restrict__ H) {
+  extern __shared__ double sm[];
+  const int n2 = n1 * n1, nq = n2 * n1, nd = nq;
+  double *w = sm;
+  double *P = w + nq;            // [cc'][q]
+  double *T1 = P + n2 * n1;      // [(q1 n1 + q2)][cc']
+  double *T2 = T1 + n2 * n2;     // [(q1 n2 + bb')][cc']
+  const int64_t e = blockIdx.x;
+  for (int q = threadIdx.x; q < nq; q += blockDim.x) w[q] = vks[e * nq + q] * jxw[e * nq + q];
+  for (int t = threadIdx.x; t < n2 * n1; t += blockDim.x) {
+    const int cc = t / n1, q = t % n1;
+    P[t] = phi[q * n1 + cc / n1] * phi[q * n1 + cc % n1];
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < n2 * n2; t += blockDim.x) {
+    const int q12 = t / n2, cc = t % n2, q1 = q12 / n1, q2 = q12 % n1;
+    double s = 0.0;
+    for (int q3 = 0; q3 < n1; ++q3) s = fma(P[cc * n1 + q3], w[q1 + n1 * q2 + n2 * q3], s);
+    T1[t] = s;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < n1 * n2 * n2; t += blockDim.x) {
+    const int cc = t % n2, r = t / n2, bb = r % n2, q1 = r / n2;
+    double s = 0.0;
+    for (int q2 = 0; q2 < n1; ++q2) s = fma(P[bb * n1 + q2], T1[(q1 * n1 + q2) * n2 + cc], s);
+    T2[t] = s;
+  }
+  __syncthreads();
+  const double hh = 0.5 * cell_h[e];
+  double *He = H + e * (int64_t)nd * nd;
+  for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) {
+    const int j = t / nd, i = t % nd;
+    const int a = i % n1, b = (i / n1) % n1, c = i / n2;
+    const int ap = j % n1, bp = (j / n1) % n1, cp = j / n2;
+    const int aa = a * n1 + ap, bb = b * n1 + bp, cc = c * n1 + cp;
+    double s = 0.0;
+    for (int q1 = 0; q1 < n1; ++q1) s = fma(P[aa * n1 + q1], T2[(q1 * n2 + bb) * n2 + cc], s);
+    He[t] = fma(hh, Kref[t], s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// HX, part 1: Y_e = H_e X_e with the constrained gather fused in.
+// One CTA per cell; thread i owns row i and BC accumulators.
+// ---------------------------------------------------------------------------
+template <int BC>
+__global__ void __launch_bounds__(NT) hx_cell_gemm_kernel(FeView fe, const double *__restrict__ H,
+                                                          const double *__restrict__ x,
+                                                          double *__restrict__ Ycell, int B,
+                                                          int mode) {
+  extern __shared__ double xs[];  // [nd][BC]
+  const int nd = fe.nd;
+  const int64_t e = blockIdx.x;
+  for (int idx = threadIdx.x; idx < nd * BC; idx += blockDim.x) {
+    const int l = idx / BC, b = idx - l * BC;
+    double v = 0.0;
+    if (b < B) {
+      if (mode == GATHER_PLAIN) {
+        const int m = fe.cell_nodes[e * nd + l];
+        v = x[(int64_t)m * B + b];
+      } else {
+        const int m = fe.cell_map[e * nd + l];
+        if (m >= 0) {
+          v = x[(int64_t)m * B + b] * fe.inv_sqrt_mass[m];
+        } else {
+          const int r = -m - 1;
+          for (int k = fe.cons_ptr[r]; k < fe.cons_ptr[r + 1]; ++k)
+            v = fma(fe.cons_gw[k], x[(int64_t)fe.cons_masters[k] * B + b], v);
+        }
+      }
+    }
+    xs[idx] = v;
+  }
+  __syncthreads();
+  const int i = threadIdx.x;
+  double acc[BC];
+#pragma unroll
+  for (int b = 0; b < BC; ++b) acc[b] = 0.0;
+  if (i < nd) {
+    const double *Hc = H + e * (int64_t)nd * nd + i;
+#pragma unroll 4
+    for (int j = 0; j < nd; ++j) {
+      const double h = __ldcs(Hc + (int64_t)j * nd);
+      const double *xr = xs + j * BC;
+#pragma unroll
+      for (int b = 0; b < BC; b += 2) {
+        const double2 xv = *reinterpret_cast<const double2 *>(xr + b);
+        acc[b] = fma(h, xv.x, acc[b]);
+        acc[b + 1] = fma(h, xv.y, acc[b + 1]);
+      }
+    }
+  }
+  __syncthreads();
+  if (i < nd) {
+#pragma unroll
+    for (int b = 0; b < BC; ++b)
+      if (b < B) xs[i * B + b] = acc[b];
+  }
+  __syncthreads();
+  double *yo = Ycell + e * (int64_t)nd * B;
+  for (int idx = threadIdx.x; idx < nd * B; idx += blockDim.x) yo[idx] = xs[idx];
+}
+
+// ---------------------------------------------------------------------------
+// HX, part 2: deterministic assembly over the node CSR + fused epilogue.
+// Thread layout (rr, j): j = column, rr = row lane; RR = NT / B rows in flight.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) hx_assemble_kernel(FeView fe, const double *__restrict__ Ycell,
+                                                         double *__restrict__ out, int B,
+                                                         AsmEpilogue epi, int64_t rows_per_block) {
+  __shared__ double red[NT];
+  const int RR = NT / B;
+  const int j = threadIdx.x % B, rr = threadIdx.x / B;
+  const int64_t r0 = blockIdx.x * rows_per_block;
+  const int64_t r1 = min(fe.nnodes, r0 + rows_per_block);
+  double dot = 0.0;
+  if (rr < RR) {
+    for (int64_t n = r0 + rr; n < r1; n += RR) {
+      double acc = 0.0;
+      for (int k = fe.sc_ptr[n]; k < fe.sc_ptr[n + 1]; ++k)
+        acc = fma(fe.sc_w[k], Ycell[(int64_t)fe.sc_src[k] * B + j], acc);
+      acc *= fe.inv_sqrt_mass[n];
+      const int64_t idx = n * B + j;
+      switch (epi.kind) {
+        case AsmEpilogue::STORE: out[idx] = acc; break;
+        case AsmEpilogue::CHEB: {
+          double v = epi.alpha * (acc - epi.c * epi.in[idx]);
+          if (epi.prev) v -= epi.beta * epi.prev[idx];
+          out[idx] = v;
+          break;
+        }
+        case AsmEpilogue::VMULT: out[idx] = acc - epi.eps[j] * epi.in[idx]; break;
+        case AsmEpilogue::RHS: {
+          double v = 0.0;
+          if (fe.sc_ptr[n + 1] > fe.sc_ptr[n] && fe.inv_sqrt_mass[n] != 0.0) {
+            double mu = 0.0;
+            for (int k = 0; k < B; ++k) mu = fma(epi.Mu[k * B + j], epi.psi[n * B + k], mu);
+            v = epi.occ4[j] * acc - 2.0 * fe.sqrt_mass[n] * mu;
+          }
+          out[idx] = v;
+          break;
+        }
+        case AsmEpilogue::MINRES: {
+          const double vv = epi.in[idx];
+          const double yn = acc - epi.eps[j] * vv - epi.minres_coef[j] * epi.prev[idx];
+          out[idx] = yn;
+          dot = fma(vv, yn, dot);
+          break;
+        }
+      }
+    }
+  }
+  if (epi.kind == AsmEpilogue::MINRES) {
+    red[threadIdx.x] = dot;
+    __syncthreads();
+    if (threadIdx.x < B) {
+      double s = 0.0;
+      for (int q = 0; q < RR; ++q) s += red[q * B + threadIdx.x];
+      epi.dot_partial[(int64_t)blockIdx.x * B + threadIdx.x] = s;
+    }
+  }
+}
+
+__global__ void scale_rows_kernel(const double *d, const double *x, double *y, int64_t n, int B) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx < n * B) y[idx] = d[idx / B] * x[idx];
+}
+
+__global__ void distribute_kernel(const int *rows, const int *ptr, const int *masters, const double *w,
+                                  int nrows, double *x, int B) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)nrows * B) return;
+  const int r = (int)(idx / B), b = (int)(idx % B);
+  double v = 0.0;
+  for (int k = ptr[r]; k < ptr[r + 1]; ++k) v = fma(w[k], x[(int64_t)masters[k] * B + b], v);
+  x[(int64_t)rows[r] * B + b] = v;
+}
+
+__global__ void set_zero_kernel(const int *rows, int nrows, double *x, int B) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)nrows * B) return;
+  x[(int64_t)rows[idx / B] * B + idx % B] = 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// Tall-skinny products
+// ---------------------------------------------------------------------------
+template <int K>
+__global__ void __launch_bounds__(NT) gram_kernel(const double *__restrict__ A, const double *__restrict__ Bm,
+                                                  int64_t n, int N, int64_t rows_per_block,
+                                                  double *__restrict__ partial) {
+  __shared__ double As[32 * 64], Bs[32 * 64];
+  const int64_t r0 = blockIdx.x * rows_per_block;
+  const int64_t r1 = min(n, r0 + rows_per_block);
+  double acc[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = 0.0;
+  for (int64_t rb = r0; rb < r1; rb += 32) {
+    const int nr = (int)min((int64_t)32, r1 - rb);
+    for (int idx = threadIdx.x; idx < nr * N; idx += blockDim.x) {
+      As[idx] = A[rb * N + idx];
+      Bs[idx] = Bm[rb * N + idx];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int o = threadIdx.x + k * NT;
+      if (o < N * N) {
+        const int i = o / N, jj = o % N;
+        double s = 0.0;
+        for (int r = 0; r < nr; ++r) s = fma(As[r * N + i], Bs[r * N + jj], s);
+        acc[k] += s;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int o = threadIdx.x + k * NT;
+    if (o < N * N) partial[(int64_t)blockIdx.x * N * N + o] = acc[k];
+  }
+}
+
+__global__ void reduce_partials_kernel(const double *partial, int nparts, int width, double *out) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= width) return;
+  double s = 0.0;
+  for (int g = 0; g < nparts; ++g) s += partial[(int64_t)g * width + o];
+  out[o] = s;
+}
+
+__global__ void __launch_bounds__(NT) rotate_kernel(const double *__restrict__ Y, const double *__restrict__ T,
+                                                    double *__restrict__ Z, int64_t n, int N) {
+  __shared__ double Ts[64 * 64];
+  for (int i = threadIdx.x; i < N * N; i += blockDim.x) Ts[i] = T[i];
+  __syncthreads();
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= n * N) return;
+  const int64_t r = idx / N;
+  const int j = (int)(idx % N);
+  const double *yr = Y + r * N;
+  double s = 0.0;
+  for (int k = 0; k < N; ++k) s = fma(yr[k], Ts[k * N + j], s);
+  Z[idx] = s;
+}
+
+__global__ void __launch_bounds__(NT) rotate_residual_kernel(const double *__restrict__ Y,
+                                                             const double *__restrict__ HY,
+                                                             const double *__restrict__ Q,
+                                                             const double *__restrict__ eps,
+                                                             double *__restrict__ X, int64_t n, int N,
+                                                             int64_t rows_per_block,
+                                                             double *__restrict__ partial) {
+  __shared__ double Qs[64 * 64];
+  __shared__ double red[NT];
+  for (int i = threadIdx.x; i < N * N; i += blockDim.x) Qs[i] = Q[i];
+  __syncthreads();
+  const int RR = NT / N;
+  const int j = threadIdx.x % N, rr = threadIdx.x / N;
+  const int64_t r0 = blockIdx.x * rows_per_block;
+  const int64_t r1 = min(n, r0 + rows_per_block);
+  double acc = 0.0;
+  if (rr < RR) {
+    for (int64_t r = r0 + rr; r < r1; r += RR) {
+      double xs = 0.0, hs = 0.0;
+      for (int k = 0; k < N; ++k) {
+        xs = fma(Y[r * N + k], Qs[k * N + j], xs);
+        hs = fma(HY[r * N + k], Qs[k * N + j], hs);
+      }
+      X[r * N + j] = xs;
+      const double res = hs - eps[j] * xs;
+      acc = fma(res, res, acc);
+    }
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x < N) {
+    double s = 0.0;
+    for (int q = 0; q < RR; ++q) s += red[q * N + threadIdx.x];
+    partial[(int64_t)blockIdx.x * N + threadIdx.x] = s;
+  }
+}
+
+__global__ void __launch_bounds__(NT) coldot_kernel(const double *__restrict__ a, const double *__restrict__ b,
+                                                    int64_t n, int B, int64_t rows_per_block,
+                                                    double *__restrict__ partial) {
+  __shared__ double red[NT];
+  const int RR = NT / B;
+  const int j = threadIdx.x % B, rr = threadIdx.x / B;
+  const int64_t r0 = blockIdx.x * rows_per_block;
+  const int64_t r1 = min(n, r0 + rows_per_block);
+  double acc = 0.0;
+  if (rr < RR)
+    for (int64_t r = r0 + rr; r < r1; r += RR) acc = fma(a[r * B + j], b[r * B + j], acc);
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x < B) {
+    double s = 0.0;
+    for (int q = 0; q < RR; ++q) s += red[q * B + threadIdx.x];
+    partial[(int64_t)blockIdx.x * B + threadIdx.x] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Cell-local interpolation kernels (column chunks of CH)
+// ---------------------------------------------------------------------------
+constexpr int CH = 16;
+
+__global__ void __launch_bounds__(NT) interp_to_quad_kernel(FeView fe, const double *__restrict__ x,
+                                                            double *__restrict__ out, int B) {
+  extern __shared__ double sm[];
+  const int n1 = fe.n1, nd = fe.nd;
+  double *A = sm;
+  double *b0 = A + n1 * n1, *b1 = b0 + nd * CH, *b2 = b1 + nd * CH;
+  for (int i = threadIdx.x; i < n1 * n1; i += blockDim.x) A[i] = fe.phi[i];
+  const int64_t e = blockIdx.x;
+  for (int c0 = 0; c0 < B; c0 += CH) {
+    const int w = min(CH, B - c0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nd * CH; idx += blockDim.x) {
+      const int l = idx / CH, k = idx % CH;
+      b0[idx] = (k < w) ? x[(int64_t)fe.cell_nodes[e * nd + l] * B + c0 + k] : 0.0;
+    }
+    __syncthreads();
+    tensor3(A, false, b0, b1, b2, n1, CH);
+    for (int idx = threadIdx.x; idx < nd * CH; idx += blockDim.x) {
+      const int q = idx / CH, k = idx % CH;
+      if (k < w) out[(e * nd + q) * B + c0 + k] = b1[idx];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(NT) r_cell_kernel(FeView fe, const double *__restrict__ x,
+                                                    const double *__restrict__ wq, double *__restrict__ Ycell,
+                                                    int B) {
+  extern __shared__ double sm[];
+  const int n1 = fe.n1, nd = fe.nd;
+  double *A = sm;
+  double *b0 = A + n1 * n1, *b1 = b0 + nd * CH, *b2 = b1 + nd * CH;
+  for (int i = threadIdx.x; i < n1 * n1; i += blockDim.x) A[i] = fe.phi[i];
+  const int64_t e = blockIdx.x;
+  for (int c0 = 0; c0 < B; c0 += CH) {
+    const int w = min(CH, B - c0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nd * CH; idx += blockDim.x) {
+      const int l = idx / CH, k = idx % CH;
+      b0[idx] = (k < w) ? x[(int64_t)fe.cell_nodes[e * nd + l] * B + c0 + k] : 0.0;
+    }
+    __syncthreads();
+    tensor3(A, false, b0, b1, b2, n1, CH);
+    for (int idx = threadIdx.x; idx < nd * CH; idx += blockDim.x) b1[idx] *= wq[e * nd + idx / CH];
+    __syncthreads();
+    tensor3(A, true, b1, b0, b2, n1, CH);
+    for (int idx = threadIdx.x; idx < nd * CH; idx += blockDim.x) {
+      const int l = idx / CH, k = idx % CH;
+      if (k < w) Ycell[(e * nd + l) * B + c0 + k] = b0[idx];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(NT) density_kernel(FeView fe, const double *__restrict__ psi,
+                                                     const double *__restrict__ occ, int N,
+                                                     const double *__restrict__ rho_t,
+                                                     const double *__restrict__ weight,
+                                                     const double *__restrict__ jxw,
+                                                     const double *__restrict__ vks, double *__restrict__ rho,
+                                                     double *__restrict__ u, double *__restrict__ partial4) {
+  extern __shared__ double sm[];
+  const int n1 = fe.n1, nd = fe.nd, nq = fe.nq;
+  double *A = sm;
+  double *b0 = A + n1 * n1, *b1 = b0 + nd * CH, *b2 = b1 + nd * CH, *rs = b2 + nd * CH;
+  __shared__ double red[32];
+  for (int i = threadIdx.x; i < n1 * n1; i += blockDim.x) A[i] = fe.phi[i];
+  for (int q = threadIdx.x; q < nq; q += blockDim.x) rs[q] = 0.0;
+  const int64_t e = blockIdx.x;
+  for (int c0 = 0; c0 < N; c0 += CH) {
+    const int w = min(CH, N - c0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nd * CH; idx += blockDim.x) {
+      const int l = idx / CH, k = idx % CH;
+      b0[idx] = (k < w) ? psi[(int64_t)fe.cell_nodes[e * nd + l] * N + c0 + k] : 0.0;
+    }
+    __syncthreads();
+    tensor3(A, false, b0, b1, b2, n1, CH);
+    for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+      double s = rs[q];
+      for (int k = 0; k < w; ++k) {
+        const double v = b1[q * CH + k];
+        s = fma(2.0 * occ[c0 + k] * v, v, s);
+      }
+      rs[q] = s;
+    }
+  }
+  __syncthreads();
+  double pl = 0.0, plu = 0.0, pl1 = 0.0, piv = 0.0;
+  for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+    const int64_t g = e * nq + q;
+    const double r = rs[q];
+    const double d = rho_t[g] - 0.5 * r;
+    rho[g] = r;
+    u[g] = d * weight[g];
+    pl += d * d * weight[g] * jxw[g];
+    plu += d * d * jxw[g];
+    pl1 += fabs(d * jxw[g]);
+    piv += vks[g] * r * jxw[g];
+  }
+  pl = block_sum<NT>(pl, red);
+  plu = block_sum<NT>(plu, red);
+  pl1 = block_sum<NT>(pl1, red);
+  piv = block_sum<NT>(piv, red);
+  if (threadIdx.x == 0) {
+    partial4[e * 4 + 0] = pl;
+    partial4[e * 4 + 1] = plu;
+    partial4[e * 4 + 2] = pl1;
+    partial4[e * 4 + 3] = piv;
+  }
+}
+
+__global__ void __launch_bounds__(NT) pair_quad_sums_kernel(int nq, const double *__restrict__ Qa,
+                                                            const double *__restrict__ Qb,
+                                                            const double *__restrict__ w, int B,
+                                                            const int *__restrict__ pairs, int npairs,
+                                                            double *__restrict__ partial) {
+  const int64_t e = blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int k = warp; k < npairs; k += nw) {
+    const int i = pairs[2 * k], j = pairs[2 * k + 1];
+    double s = 0.0;
+    for (int q = lane; q < nq; q += 32) {
+      const int64_t g = e * nq + q;
+      s = fma(w[g] * Qa[g * B + i], Qb[g * B + j], s);
+    }
+    s = warp_sum(s);
+    if (lane == 0) partial[e * npairs + k] = s;
+  }
+}
+
+__global__ void nullspace_update_kernel(double *x, const double *psi, int64_t n, int B, const int *pair_ptr,
+                                        const int *pair_j, const double *coef) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= n * B) return;
+  const int64_t r = idx / B;
+  const int i = (int)(idx % B);
+  double acc = x[idx];
+  for (int k = pair_ptr[i]; k < pair_ptr[i + 1]; ++k) acc = fma(coef[k], psi[r * B + pair_j[k]], acc);
+  x[idx] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// MINRES kernels (per-column masks; scalars live on the device)
+// ---------------------------------------------------------------------------
+__global__ void minres_v_kernel(const double *y, const double *beta, double *v, int64_t n, int B) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= n * B) return;
+  const double bt = beta[idx % B];
+  v[idx] = bt > 0.0 ? y[idx] / bt : 0.0;
+}
+
+__global__ void __launch_bounds__(NT) minres_init_kernel(const double *__restrict__ b, const double *__restrict__ diagA,
+                                                         double *r1, double *r2, double *y, int64_t n, int B,
+                                                         int64_t rows_per_block, double *partial) {
+  __shared__ double red[NT];
+  const int RR = NT / B;
+  const int j = threadIdx.x % B, rr = threadIdx.x / B;
+  const int64_t r0 = blockIdx.x * rows_per_block;
+  const int64_t r1e = min(n, r0 + rows_per_block);
+  double acc = 0.0;
+  if (rr < RR)
+    for (int64_t r = r0 + rr; r < r1e; r += RR) {
+      const int64_t idx = r * B + j;
+      const double bv = b[idx];
+      const double yv = diagA[r] * bv;
+      r1[idx] = bv;
+      r2[idx] = bv;
+      y[idx] = yv;
+      acc = fma(bv, yv, acc);
+    }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x < B) {
+    double s = 0.0;
+    for (int q = 0; q < RR; ++q) s += red[q * B + threadIdx.x];
+    partial[(int64_t)blockIdx.x * B + threadIdx.x] = s;
+  }
+}
+
+__global__ void minres_init_scalars_kernel(MinresState st, const double *beta1_sq, int B) {
+  const int b = threadIdx.x;
+  if (b >= B) return;
+  const double b1 = sqrt(fmax(beta1_sq[b], 0.0));
+  st.beta[b] = b1;
+  st.oldb[b] = 0.0;
+  st.dbar[b] = 0.0;
+  st.epsln[b] = 0.0;
+  st.phibar[b] = b1;
+  st.cs[b] = -1.0;
+  st.sn[b] = 0.0;
+  st.coef1[b] = 0.0;
+  st.active[b] = (b1 >= st.tol) ? 1 : 0;
+  st.commit[b] = 0;
+  st.iters[b] = 0;
+}
+
+__global__ void __launch_bounds__(NT) minres_update1_kernel(double *__restrict__ r1, double *__restrict__ r2,
+                                                            double *__restrict__ y, const double *__restrict__ yn,
+                                                            const double *__restrict__ diagA, MinresState st,
+                                                            int64_t n, int B, int64_t rows_per_block,
+                                                            double *__restrict__ partial) {
+  __shared__ double red[NT];
+  const int RR = NT / B;
+  const int j = threadIdx.x % B, rr = threadIdx.x / B;
+  const int64_t r0 = blockIdx.x * rows_per_block;
+  const int64_t r1e = min(n, r0 + rows_per_block);
+  double acc = 0.0;
+  if (rr < RR && st.active[j]) {
+    const double a = st.alfa[j] / st.beta[j];
+    for (int64_t r = r0 + rr; r < r1e; r += RR) {
+      const int64_t idx = r * B + j;
+      const double r2o = r2[idx];
+      const double ynv = yn[idx] - a * r2o;
+      const double yv = diagA[r] * ynv;
+      r1[idx] = r2o;
+      r2[idx] = ynv;
+      y[idx] = yv;
+      acc = fma(ynv, yv, acc);
+    }
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x < B) {
+    double s = 0.0;
+    for (int q = 0; q < RR; ++q) s += red[q * B + threadIdx.x];
+    partial[(int64_t)blockIdx.x * B + threadIdx.x] = s;
+  }
+}
+
+__global__ void minres_scalars_kernel(MinresState st, int B) {
+  const int b = threadIdx.x;
+  if (b >= B) return;
+  if (!st.active[b]) {
+    st.commit[b] = 0;
+    return;
+  }
+  const double beta = st.beta[b];
+  const double betan = sqrt(fmax(st.beta2[b], 0.0));
+  const double alfa = st.alfa[b];
+  const double cs = st.cs[b], sn = st.sn[b], dbar = st.dbar[b];
+  const double oldeps = st.epsln[b];
+  const double delta = cs * dbar + sn * alfa;
+  const double gbar = sn * dbar - cs * alfa;
+  const double epsln = sn * betan;
+  const double dbarn = -cs * betan;
+  double gamma = sqrt(gbar * gbar + betan * betan);
+  gamma = fmax(gamma, 2.220446049250313e-16);
+  const double csn = gbar / gamma, snn = betan / gamma;
+  const double phibar = st.phibar[b];
+  const double phi = csn * phibar;
+  const double phibarn = snn * phibar;
+  st.oldb[b] = beta;
+  st.beta[b] = betan;
+  st.epsln[b] = epsln;
+  st.dbar[b] = dbarn;
+  st.cs[b] = csn;
+  st.sn[b] = snn;
+  st.phibar[b] = phibarn;
+  st.oldeps[b] = oldeps;
+  st.delta[b] = delta;
+  st.denom[b] = 1.0 / gamma;
+  st.phi[b] = phi;
+  st.coef1[b] = beta > 0.0 ? betan / beta : 0.0;
+  st.commit[b] = 1;
+  st.iters[b] += 1;
+  st.active[b] = (phibarn >= st.tol) ? 1 : 0;
+}
+
+__global__ void minres_update2_kernel(double *__restrict__ x, double *__restrict__ w, double *__restrict__ w2,
+                                      const double *__restrict__ v, MinresState st, int64_t n, int B) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= n * B) return;
+  const int b = (int)(idx % B);
+  if (!st.commit[b]) return;
+  const double wo = w[idx], w2o = w2[idx];
+  const double wn = (v[idx] - st.oldeps[b] * w2o - st.delta[b] * wo) * st.denom[b];
+  w2[idx] = wo;
+  w[idx] = wn;
+  x[idx] = fma(st.phi[b], wn, x[idx]);
+}
+
+// ---------------------------------------------------------------------------
+// Child mesh transfers
+// ---------------------------------------------------------------------------
+__global__ void child_to_parent_quad_kernel(ChildView cv, const double *__restrict__ pot,
+                                            const double *__restrict__ v_base,
+                                            const double *__restrict__ v_lda, double factor_lda,
+                                            double *__restrict__ vks, int64_t nqtot) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q >= nqtot) return;
+  const int c = cv.pq_child[q];
+  const double x = cv.pq_xi[3 * q], y = cv.pq_xi[3 * q + 1], z = cv.pq_xi[3 * q + 2];
+  const int *nodes = cv.cell_nodes + (int64_t)c * 8;
+  double v = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const double wx = (k & 1) ? x : 1.0 - x;
+    const double wy = (k & 2) ? y : 1.0 - y;
+    const double wz = (k & 4) ? z : 1.0 - z;
+    v = fma(wx * wy * wz, pot[nodes[k]], v);
+  }
+  vks[q] = v_base[q] + v + factor_lda * v_lda[q];
+}
+
+// One CTA per work item (parent cell, range of its child cells); one warp per
+// child cell; lane = state column.  S[c*8+q] += sum_i psi_i(q) p_i(q).
+__global__ void __launch_bounds__(NT) psi_adjoint_child_kernel(FeView fe, ChildView cv,
+                                                               const double *__restrict__ psi,
+                                                               const double *__restrict__ p, int B,
+                                                               double *__restrict__ S) {
+  extern __shared__ double sm[];
+  const int n1 = fe.n1, nd = fe.nd, n2 = n1 * n1;
+  double *Us = sm;                  // [nd][32]
+  double *Ps = Us + nd * 32;        // [nd][32]
+  double *gl = Ps + nd * 32;        // [n1] GLL nodes
+  double *inv = gl + n1;            // [n1] inverse denominators
+  double *Lw = inv + n1;            // per warp [3][2][n1]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int e = cv.work_parent[blockIdx.x];
+  const int c0 = cv.work_c0[blockIdx.x], c1 = cv.work_c1[blockIdx.x];
+  if (threadIdx.x < n1) {
+    const double xa = cv.gll[threadIdx.x];
+    double d = 1.0;
+    for (int b = 0; b < n1; ++b)
+      if (b != (int)threadIdx.x) d *= (xa - cv.gll[b]);
+    gl[threadIdx.x] = xa;
+    inv[threadIdx.x] = 1.0 / d;
+  }
+  double *L = Lw + warp * 6 * n1;
+  for (int cb = 0; cb < B; cb += 32) {
+    const int wcols = min(32, B - cb);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nd * 32; idx += blockDim.x) {
+      const int l = idx >> 5, k = idx & 31;
+      const int64_t node = fe.cell_nodes[(int64_t)e * nd + l];
+      Us[idx] = (k < wcols) ? psi[node * B + cb + k] : 0.0;
+      Ps[idx] = (k < wcols) ? p[node * B + cb + k] : 0.0;
+    }
+    __syncthreads();
+    for (int c = c0 + warp; c < c1; c += nw) {
+      for (int t = lane; t < 6 * n1; t += 32) {
+        const int dim = t / (2 * n1), pt = (t / n1) % 2, a = t % n1;
+        const double xi = cv.offset[(int64_t)c * 3 + dim] + cv.scale[c] * cv.g2[pt];
+        double v = inv[a];
+        for (int b = 0; b < n1; ++b)
+          if (b != a) v *= (xi - gl[b]);
+        L[t] = v;   // L[(dim*2 + pt)*n1 + a]
+      }
+      __syncwarp();
+      const double *Lx = L, *Ly = L + 2 * n1, *Lz = L + 4 * n1;
+      double op[8], oa[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) { op[q] = 0.0; oa[q] = 0.0; }
+      for (int cz = 0; cz < n1; ++cz) {
+        double tp[4] = {0, 0, 0, 0}, ta[4] = {0, 0, 0, 0};
+        for (int by = 0; by < n1; ++by) {
+          double xp0 = 0, xp1 = 0, xa0 = 0, xa1 = 0;
+          const int base = (n1 * by + n2 * cz) * 32 + lane;
+          for (int a = 0; a < n1; ++a) {
+            const double uv = Us[base + a * 32], pv = Ps[base + a * 32];
+            xp0 = fma(Lx[a], uv, xp0);
+            xp1 = fma(Lx[n1 + a], uv, xp1);
+            xa0 = fma(Lx[a], pv, xa0);
+            xa1 = fma(Lx[n1 + a], pv, xa1);
+          }
+          const double ly0 = Ly[by], ly1 = Ly[n1 + by];
+          tp[0] = fma(ly0, xp0, tp[0]); tp[1] = fma(ly0, xp1, tp[1]);
+          tp[2] = fma(ly1, xp0, tp[2]); tp[3] = fma(ly1, xp1, tp[3]);
+          ta[0] = fma(ly0, xa0, ta[0]); ta[1] = fma(ly0, xa1, ta[1]);
+          ta[2] = fma(ly1, xa0, ta[2]); ta[3] = fma(ly1, xa1, ta[3]);
+        }
+        const double lz0 = Lz[cz], lz1 = Lz[n1 + cz];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          op[q] = fma(lz0, tp[q], op[q]);
+          op[4 + q] = fma(lz1, tp[q], op[4 + q]);
+          oa[q] = fma(lz0, ta[q], oa[q]);
+          oa[4 + q] = fma(lz1, ta[q], oa[4 + q]);
+        }
+      }
+      double prod[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) prod[q] = warp_sum(lane < wcols ? op[q] * oa[q] : 0.0);
+      if (lane < 8) {
+        double pv = prod[0];
+#pragma unroll
+        for (int q = 1; q < 8; ++q)
+          if (lane == q) pv = prod[q];
+        S[(int64_t)c * 8 + lane] += pv;
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__global__ void force_project_kernel(ChildView cv, const double *__restrict__ S, double *__restrict__ force) {
+  const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (n >= cv.nchild_nodes) return;
+  const double g0 = cv.g2[0], g1 = cv.g2[1];
+  double f = 0.0;
+  for (int k = cv.sc_ptr[n]; k < cv.sc_ptr[n + 1]; ++k) {
+    const int src = cv.sc_src[k];
+    const int c = src >> 3, kk = src & 7;
+    double loc = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const double gx = (q & 1) ? g1 : g0, gy = (q & 2) ? g1 : g0, gz = (q & 4) ? g1 : g0;
+      const double nk = ((kk & 1) ? gx : 1.0 - gx) * ((kk & 2) ? gy : 1.0 - gy) * ((kk & 4) ? gz : 1.0 - gz);
+      const int64_t g = (int64_t)c * 8 + q;
+      loc = fma(nk * cv.jxw[g], S[g], loc);
+    }
+    f = fma(cv.sc_w[k], loc, f);
+  }
+  force[n] = f;
+}
+
+std::atomic<long long> g_launches{0};
+
+int pick_blocks(int64_t rows, int64_t min_rows) {
+  int64_t nb = (rows + min_rows - 1) / min_rows;
+  if (nb > 148 * 8) nb = 148 * 8;
+  if (nb < 1) nb = 1;
+  return (int)nb;
+}
+
+}  // namespace
+
+long long launch_count() { return g_launches.load(); }
+void count_launch() { g_launches.fetch_add(1); }
+
+// ---------------------------------------------------------------------------
+// launch wrappers (each counts its launches)
+// ---------------------------------------------------------------------------
+#undef INVDFT_LAUNCH_CHECK
+#define INVDFT_LAUNCH_CHECK()              \
+  do {                                     \
+    g_launches.fetch_add(1);               \
+    INVDFT_CUDA(cudaGetLastError());       \
+  } while (0)
+void launch_build_cell_h(const FeView &fe, const double *vks, const double *jxw, const double *Kref,
+                         double *H, cudaStream_t s) {
+  const int n1 = fe.n1, n2 = n1 * n1;
+  const size_t smem = sizeof(double) * (size_t)(n2 * n1 + n2 * n1 + n2 * n2 + n1 * n2 * n2);
+  static bool attr = false;
+  if (!attr) {
+    INVDFT_CUDA(cudaFuncSetAttribute(build_cell_h_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr = true;
+  }
+  build_cell_h_kernel<<<(unsigned)fe.nc, NT, smem, s>>>(n1, fe.phi, vks, jxw, Kref, fe.cell_h, H);
+  INVDFT_LAUNCH_CHECK();
+}
+
+template <int BC>
+static void hx_gemm_bc(const FeView &fe, const double *H, const double *x, double *Ycell, int B, int mode,
+                       cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_cell_gemm_kernel<BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     200 * 1024));
+    attr = true;
+  }
+  const int threads = ((fe.nd + 31) / 32) * 32;
+  if (threads > NT) throw StatusError(5, "cell too large for the FP64 HX kernel");
+  const size_t smem = sizeof(double) * (size_t)fe.nd * BC;
+  hx_cell_gemm_kernel<BC><<<(unsigned)fe.nc, threads, smem, s>>>(fe, H, x, Ycell, B, mode);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_hx_cell_gemm(const FeView &fe, const double *H, const double *x, double *Ycell, int B,
+                         int gather_mode, cudaStream_t s) {
+  if (B <= 2) hx_gemm_bc<2>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 4) hx_gemm_bc<4>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 8) hx_gemm_bc<8>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 16) hx_gemm_bc<16>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 32) hx_gemm_bc<32>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 64) hx_gemm_bc<64>(fe, H, x, Ycell, B, gather_mode, s);
+  else throw StatusError(5, "block width above 64");
+}
+
+void launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B, const AsmEpilogue &epi,
+                        int dot_blocks, cudaStream_t s) {
+  if (B > NT) throw StatusError(5, "block width above 256");
+  const int nb = dot_blocks > 0 ? dot_blocks : pick_blocks(fe.nnodes, 64);
+  const int64_t rpb = (fe.nnodes + nb - 1) / nb;
+  hx_assemble_kernel<<<nb, NT, 0, s>>>(fe, Ycell, out, B, epi, rpb);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_scale_rows(const double *d, const double *x, double *y, int64_t n, int B, cudaStream_t s) {
+  if (n * B == 0) return;
+  scale_rows_kernel<<<ceil_div(n * B, NT), NT, 0, s>>>(d, x, y, n, B);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_distribute(const int *rows, const int *ptr, const int *masters, const double *w, int nrows,
+                       double *x, int B, cudaStream_t s) {
+  if ((int64_t)nrows * B == 0) return;
+  distribute_kernel<<<ceil_div((int64_t)nrows * B, NT), NT, 0, s>>>(rows, ptr, masters, w, nrows, x, B);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_set_zero(const int *rows, int nrows, double *x, int B, cudaStream_t s) {
+  if ((int64_t)nrows * B == 0) return;
+  set_zero_kernel<<<ceil_div((int64_t)nrows * B, NT), NT, 0, s>>>(rows, nrows, x, B);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_reduce_partials(const double *partial, int nparts, int width, double *out, cudaStream_t s) {
+  reduce_partials_kernel<<<ceil_div(width, NT), NT, 0, s>>>(partial, nparts, width, out);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_gram(const double *A, const double *Bm, int64_t n, int N, double *partial, int nblocks,
+                 double *out, cudaStream_t s) {
+  if (N > 64) throw StatusError(5, "subspace wider than 64");
+  const int64_t rpb = (n + nblocks - 1) / nblocks;
+  const int K = (N * N + NT - 1) / NT;
+  if (K <= 1) gram_kernel<1><<<nblocks, NT, 0, s>>>(A, Bm, n, N, rpb, partial);
+  else if (K <= 4) gram_kernel<4><<<nblocks, NT, 0, s>>>(A, Bm, n, N, rpb, partial);
+  else gram_kernel<16><<<nblocks, NT, 0, s>>>(A, Bm, n, N, rpb, partial);
+  INVDFT_LAUNCH_CHECK();
+  launch_reduce_partials(partial, nblocks, N * N, out, s);
+}
+
+void launch_rotate(const double *Y, const double *T, double *Z, int64_t n, int N, cudaStream_t s) {
+  rotate_kernel<<<ceil_div(n * N, NT), NT, 0, s>>>(Y, T, Z, n, N);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_rotate_residual(const double *Y, const double *HY, const double *Q, const double *eps, double *X,
+                            int64_t n, int N, double *partial, int nblocks, double *out, cudaStream_t s) {
+  const int64_t rpb = (n + nblocks - 1) / nblocks;
+  rotate_residual_kernel<<<nblocks, NT, 0, s>>>(Y, HY, Q, eps, X, n, N, rpb, partial);
+  INVDFT_LAUNCH_CHECK();
+  launch_reduce_partials(partial, nblocks, N, out, s);
+}
+
+void launch_coldot(const double *a, const double *b, int64_t n, int B, double *partial, int nblocks,
+                   double *out, cudaStream_t s) {
+  const int64_t rpb = (n + nblocks - 1) / nblocks;
+  coldot_kernel<<<nblocks, NT, 0, s>>>(a, b, n, B, rpb, partial);
+  INVDFT_LAUNCH_CHECK();
+  launch_reduce_partials(partial, nblocks, B, out, s);
+}
+
+static size_t interp_smem(const FeView &fe, int extra) {
+  return sizeof(double) * ((size_t)fe.n1 * fe.n1 + 3 * (size_t)fe.nd * CH + extra);
+}
+
+void launch_interp_to_quad(const FeView &fe, const double *x, double *out, int B, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    INVDFT_CUDA(cudaFuncSetAttribute(interp_to_quad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr = true;
+  }
+  interp_to_quad_kernel<<<(unsigned)fe.nc, NT, interp_smem(fe, 0), s>>>(fe, x, out, B);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_pair_quad_sums(const FeView &fe, const double *Qa, const double *Qb, const double *w, int B,
+                           const int *pairs, int npairs, double *partial, cudaStream_t s) {
+  if (npairs == 0) return;
+  pair_quad_sums_kernel<<<(unsigned)fe.nc, NT, 0, s>>>(fe.nq, Qa, Qb, w, B, pairs, npairs, partial);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_r_cell(const FeView &fe, const double *x, const double *wq, double *Ycell, int B, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    INVDFT_CUDA(cudaFuncSetAttribute(r_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr = true;
+  }
+  r_cell_kernel<<<(unsigned)fe.nc, NT, interp_smem(fe, 0), s>>>(fe, x, wq, Ycell, B);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_density(const FeView &fe, const double *psi, const double *occ, int N, const double *rho_t,
+                    const double *weight, const double *jxw, const double *vks, double *rho, double *u,
+                    double *partial4, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    INVDFT_CUDA(cudaFuncSetAttribute(density_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr = true;
+  }
+  density_kernel<<<(unsigned)fe.nc, NT, interp_smem(fe, fe.nq), s>>>(fe, psi, occ, N, rho_t, weight, jxw, vks,
+                                                                     rho, u, partial4);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_nullspace_update(double *x, const double *psi, int64_t n, int B, const int *pair_ptr,
+                             const int *pair_j, const double *coef, cudaStream_t s) {
+  nullspace_update_kernel<<<ceil_div(n * B, NT), NT, 0, s>>>(x, psi, n, B, pair_ptr, pair_j, coef);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_minres_v(const double *y, const MinresState &st, double *v, int64_t n, int B, cudaStream_t s) {
+  minres_v_kernel<<<ceil_div(n * B, NT), NT, 0, s>>>(y, st.beta, v, n, B);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_minres_init(const double *b, const double *diagA, double *r1, double *r2, double *y, int64_t n,
+                        int B, double *partial, int nblocks, cudaStream_t s) {
+  const int64_t rpb = (n + nblocks - 1) / nblocks;
+  minres_init_kernel<<<nblocks, NT, 0, s>>>(b, diagA, r1, r2, y, n, B, rpb, partial);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_minres_init_scalars(const MinresState &st, const double *beta1_sq, int B, cudaStream_t s) {
+  minres_init_scalars_kernel<<<1, 64, 0, s>>>(st, beta1_sq, B);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_minres_update1(double *r1, double *r2, double *y, const double *yn, const double *diagA,
+                           const MinresState &st, int64_t n, int B, double *partial, int nblocks,
+                           cudaStream_t s) {
+  const int64_t rpb = (n + nblocks - 1) / nblocks;
+  minres_update1_kernel<<<nblocks, NT, 0, s>>>(r1, r2, y, yn, diagA, st, n, B, rpb, partial);
+  INVDFT_LAUNCH_CHECK();
+  launch_reduce_partials(partial, nblocks, B, st.beta2, s);
+}
+
+void launch_minres_scalars(const MinresState &st, int B, int itn, cudaStream_t s) {
+  (void)itn;
+  minres_scalars_kernel<<<1, 64, 0, s>>>(st, B);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_minres_update2(double *x, double *w, double *w2, const double *v, const MinresState &st,
+                           int64_t n, int B, cudaStream_t s) {
+  minres_update2_kernel<<<ceil_div(n * B, NT), NT, 0, s>>>(x, w, w2, v, st, n, B);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_child_to_parent_quad(const ChildView &cv, const double *pot, const double *v_base,
+                                 const double *v_lda, double factor_lda, double *vks, int64_t nqtot,
+                                 cudaStream_t s) {
+  child_to_parent_quad_kernel<<<ceil_div(nqtot, NT), NT, 0, s>>>(cv, pot, v_base, v_lda, factor_lda, vks, nqtot);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_psi_adjoint_child(const FeView &fe, const ChildView &cv, const double *psi, const double *p, int B,
+                              double *S, cudaStream_t s) {
+  if (cv.nwork == 0) return;
+  static bool attr = false;
+  if (!attr) {
+    INVDFT_CUDA(cudaFuncSetAttribute(psi_adjoint_child_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     200 * 1024));
+    attr = true;
+  }
+  const size_t smem = sizeof(double) * ((size_t)fe.nd * 64 + 2 * fe.n1 + (NT / 32) * 6 * fe.n1);
+  psi_adjoint_child_kernel<<<cv.nwork, NT, smem, s>>>(fe, cv, psi, p, B, S);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_force_project(const ChildView &cv, const double *S, double *force, cudaStream_t s) {
+  force_project_kernel<<<ceil_div(cv.nchild_nodes, NT), NT, 0, s>>>(cv, S, force);
+  INVDFT_LAUNCH_CHECK();
+}
+
+}  // namespace invdft

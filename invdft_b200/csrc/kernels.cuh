@@ -1,0 +1,133 @@
+// Device kernels of the force evaluation (declarations + small device helpers).
+#pragma once
+#include "common.cuh"
+
+namespace invdft {
+
+// Device-side view of the parent finite-element data.
+struct FeView {
+  int n1, nd, nq;
+  int64_t nc, nnodes;
+  const double *phi;        // [n1][n1]: phi[q*n1+a] = l_a(gauss_q)
+  const double *cell_h;     // [nc]
+  const int *cell_nodes;    // [nc*nd]
+  const int *cell_map;      // [nc*nd]: node (free) or -(1+constraint row)
+  const int *cons_ptr;      // [ncons+1]
+  const int *cons_masters;
+  const double *cons_w;     // plain weights
+  const double *cons_gw;    // weights * M^-1/2[master] (Lowdin gather)
+  const int *cons_rows;     // [ncons]
+  int ncons;
+  const int *sc_ptr;        // [nnodes+1] scatter CSR over nodes
+  const int *sc_src;        // entry -> cell*nd + local
+  const double *sc_w;       // condensation weight
+  const double *inv_sqrt_mass, *sqrt_mass;
+};
+
+// Gather modes of the cell GEMM.
+enum GatherMode { GATHER_LOWDIN = 0, GATHER_PLAIN = 1 };
+
+// ---- launches (implemented in kernels.cu) ----
+long long launch_count();  // kernels launched by this library so far
+void count_launch();       // for launches made outside kernels.cu
+void launch_build_cell_h(const FeView &fe, const double *vks, const double *jxw, const double *Kref,
+                         double *H, cudaStream_t s);
+void launch_hx_cell_gemm(const FeView &fe, const double *H, const double *x, double *Ycell, int B,
+                         int gather_mode, cudaStream_t s);
+
+// Epilogue selector for the assembly kernel.
+struct AsmEpilogue {
+  enum Kind { STORE = 0, CHEB = 1, VMULT = 2, RHS = 3, MINRES = 4 } kind = STORE;
+  double alpha = 1.0, c = 0.0, beta = 0.0;   // CHEB: out = alpha*(acc - c*in) - beta*prev
+  const double *in = nullptr;                // CHEB input block / VMULT x / MINRES v
+  const double *prev = nullptr;              // CHEB previous block / MINRES r1
+  const double *eps = nullptr;               // VMULT/MINRES shifts (eps_b, added as -eps_b x)
+  const double *occ4 = nullptr;              // RHS: 4 f_b
+  const double *Mu = nullptr;                // RHS: Mu[k*B+b]
+  const double *psi = nullptr;               // RHS: distributed nodal psi
+  const double *minres_coef = nullptr;       // MINRES: beta/oldb per column (0 at itn 1)
+  double *dot_partial = nullptr;             // MINRES: per-block column partials of v.y
+};
+void launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B,
+                        const AsmEpilogue &epi, int dot_blocks, cudaStream_t s);
+
+void launch_scale_rows(const double *d, const double *x, double *y, int64_t n, int B, cudaStream_t s);
+void launch_distribute(const int *rows, const int *ptr, const int *masters, const double *w, int nrows,
+                       double *x, int B, cudaStream_t s);
+void launch_set_zero(const int *rows, int nrows, double *x, int B, cudaStream_t s);
+
+// Tall-skinny products, deterministic: C = A^T B, N x N (N <= 64)
+void launch_gram(const double *A, const double *Bm, int64_t n, int N, double *partial, int nblocks,
+                 double *out, cudaStream_t s);
+// Z = Y T (T N x N)
+void launch_rotate(const double *Y, const double *T, double *Z, int64_t n, int N, cudaStream_t s);
+// X = Y Q, R = HY Q - X diag(eps): column sums of R^2 into out [N]
+void launch_rotate_residual(const double *Y, const double *HY, const double *Q, const double *eps,
+                            double *X, int64_t n, int N, double *partial, int nblocks, double *out,
+                            cudaStream_t s);
+// per-column dot products a.b over n rows -> out [B] (deterministic)
+void launch_coldot(const double *a, const double *b, int64_t n, int B, double *partial, int nblocks,
+                   double *out, cudaStream_t s);
+void launch_reduce_partials(const double *partial, int nparts, int width, double *out, cudaStream_t s);
+
+// Interpolation of nodal blocks to parent quadrature points: out [nc][nq][B]
+void launch_interp_to_quad(const FeView &fe, const double *x, double *out, int B, cudaStream_t s);
+// per-cell pair sums: partial[e*npairs + k] = fac(k) * sum_q w[e,q] Qa[e,q,i_k] Qb[e,q,j_k]
+void launch_pair_quad_sums(const FeView &fe, const double *Qa, const double *Qb, const double *w, int B,
+                           const int *pairs, int npairs, double *partial, cudaStream_t s);
+// sum_e R_e x_e with R_e = N^T diag(wq) N: Ycell [nc][nd][B]
+void launch_r_cell(const FeView &fe, const double *x, const double *wq, double *Ycell, int B,
+                   cudaStream_t s);
+// density rho = 2 sum f psi^2 at parent quad points + drho/u/loss partials
+void launch_density(const FeView &fe, const double *psi, const double *occ, int N, const double *rho_t,
+                    const double *weight, const double *jxw, const double *vks, double *rho,
+                    double *u, double *partial4, cudaStream_t s);
+// x[:, i] += sum_{k in pairs with i_k = i} coef_k psi[:, j_k]
+void launch_nullspace_update(double *x, const double *psi, int64_t n, int B, const int *pair_ptr,
+                             const int *pair_j, const double *coef, cudaStream_t s);
+
+// MINRES building blocks (per-column masked, scalars on device)
+struct MinresState {
+  double *beta, *oldb, *dbar, *epsln, *phibar, *cs, *sn;
+  double *alfa, *beta2;            // reduced dots
+  double *coef1;                   // beta/oldb (0 at the first iteration)
+  double *oldeps, *delta, *denom, *phi;
+  int *active, *commit, *iters;
+  double tol;
+};
+void launch_minres_v(const double *y, const MinresState &st, double *v, int64_t n, int B, cudaStream_t s);
+void launch_minres_update1(double *r1, double *r2, double *y, const double *yn, const double *diagA,
+                           const MinresState &st, int64_t n, int B, double *partial, int nblocks,
+                           cudaStream_t s);
+void launch_minres_scalars(const MinresState &st, int B, int itn, cudaStream_t s);
+void launch_minres_update2(double *x, double *w, double *w2, const double *v, const MinresState &st,
+                           int64_t n, int B, cudaStream_t s);
+void launch_minres_init(const double *b, const double *diagA, double *r1, double *r2, double *y,
+                        int64_t n, int B, double *partial, int nblocks, cudaStream_t s);
+void launch_minres_init_scalars(const MinresState &st, const double *beta1_sq, int B, cudaStream_t s);
+
+// Child mesh transfers
+struct ChildView {
+  int64_t ncc, nchild_nodes;
+  const int *cell_nodes;      // [ncc*8]
+  const double *jxw;          // [ncc*8]
+  const int *parent;          // [ncc]
+  const double *offset;       // [ncc*3]
+  const double *scale;        // [ncc]
+  const int *pq_child;        // [nc*nq]
+  const double *pq_xi;        // [nc*nq*3]
+  const int *sc_ptr, *sc_src; // scatter CSR over child nodes (entry = cell*8 + k)
+  const double *sc_w;
+  const int *work_parent, *work_c0, *work_c1; // transfer work items
+  int nwork;
+  const double *gll;          // [n1] parent GLL nodes
+  const double *g2;           // [2] Gauss points of the child rule
+};
+void launch_child_to_parent_quad(const ChildView &cv, const double *pot, const double *v_base,
+                                 const double *v_lda, double factor_lda, double *vks, int64_t nqtot,
+                                 cudaStream_t s);
+void launch_psi_adjoint_child(const FeView &fe, const ChildView &cv, const double *psi, const double *p,
+                              int B, double *S, cudaStream_t s);
+void launch_force_project(const ChildView &cv, const double *S, double *force, cudaStream_t s);
+
+}  // namespace invdft

@@ -61,6 +61,7 @@ class SystemConfig:
     unit_weights: bool = False
     child_level_cap: int = 99         # limit on child refinement (tests)
     padding: float | None = None      # cube half-width = extent + padding
+    child_extra_levels: int = 0       # refine the child mesh below the parent's minimum size
 
 
 def _ethylene():
@@ -113,14 +114,19 @@ def _octane():
     return Z, [p - ctr for p in P]
 
 
-def config(name: str) -> SystemConfig:
-    """Named workloads: c0..c4 and small test systems."""
+def config(name: str, **overrides) -> SystemConfig:
+    """Named workloads: c0..c4 and small test systems (fields overridable)."""
+    import dataclasses
+    return dataclasses.replace(_config(name), **overrides) if overrides else _config(name)
+
+
+def _config(name: str) -> SystemConfig:
     if name == "c0_lih":
         return SystemConfig("c0_lih", [3, 1], [[0, 0, 0], [0, 0, 3.0]], 4, 6, 4,
                             15.0, 0.25, 4.0, 0.5, 6, 1000)
     if name in ("c1_c2h4", "c2_c2h4"):
         Z, P = _ethylene()
-        return SystemConfig(name, Z, [list(p) for p in P], 16, 16, 5, 20.0, 0.3, 2.5,
+        return SystemConfig(name, Z, [list(p) for p in P], 16, 16, 5, 20.0, 0.32, 2.5,
                             0.35, 10, 1001 if name == "c1_c2h4" else 1002)
     if name == "c3_h2o":
         Z, P = _water()
@@ -128,14 +134,19 @@ def config(name: str) -> SystemConfig:
                             0.3, 6, 1003, unit_weights=True)
     if name == "c4_c8h18":
         Z, P = _octane()
-        return SystemConfig("c4_c8h18", Z, [list(p) for p in P], 66, 50, 5, 0.0, 0.3, 2.5,
+        return SystemConfig("c4_c8h18", Z, [list(p) for p in P], 66, 50, 5, 0.0, 0.32, 2.6,
                             0.35, 12, 1004, padding=15.0)
     if name == "tiny_h2":
         return SystemConfig("tiny_h2", [1, 1], [[-0.7, 0, 0], [0.7, 0, 0]], 2, 4, 2,
-                            6.0, 0.75, 3.0, 0.6, 4, 7, vxc_domain=2.0, child_level_cap=5)
+                            6.0, 0.75, 3.0, 0.6, 4, 7, vxc_domain=0.5, child_level_cap=6,
+                            child_extra_levels=1)
     if name == "small_lih":
         return SystemConfig("small_lih", [3, 1], [[0, 0, 0], [0, 0, 3.0]], 4, 6, 2,
                             8.0, 0.5, 4.0, 0.7, 6, 1000, vxc_domain=1.0, child_level_cap=6)
+    if name in ("tiny_h2_p4", "tiny_h2_p5"):
+        return SystemConfig(name, [1, 1], [[-0.7, 0, 0], [0.7, 0, 0]], 2, 4, int(name[-1]),
+                            6.0, 0.75, 3.0, 0.6, 4, 7, vxc_domain=1.0, child_level_cap=6,
+                            child_extra_levels=1)
     if name == "small_lih_p4":
         return SystemConfig("small_lih_p4", [3, 1], [[0, 0, 0], [0, 0, 3.0]], 4, 6, 4,
                             10.0, 0.625, 2.5, 0.5, 6, 1000, vxc_domain=3.0)
@@ -299,7 +310,7 @@ def _child_tree(cfg: SystemConfig, parent: Octree) -> Octree:
     lo = pos.min(axis=0) - cfg.vxc_domain
     hi = pos.max(axis=0) + cfg.vxc_domain
     t = parent.copy()
-    hmin = float(parent.cell_size().min())
+    hmin = float(parent.cell_size().min()) / 2 ** cfg.child_extra_levels
     cap = cfg.child_level_cap
 
     def pred(tr: Octree):
@@ -317,7 +328,9 @@ def build_problem(cfg: SystemConfig | str, target_solver=None, vxc_target=None) 
 
     ``target_solver(problem, v_ks_quad) -> (psi_nodal [n_nodes, N], eig [N],
     occ [N])`` produces the forward ground state used for rho*; by default a
-    dense eigensolve (small problems only).
+    dense eigensolve (small problems only).  ``target_solver="atoms"`` takes
+    rho* = the superposition of the atomic clouds instead (no forward solve;
+    the target is then not exactly reachable, which parity checks do not need).
     """
     if isinstance(cfg, str):
         cfg = config(cfg)
@@ -384,6 +397,9 @@ def build_problem(cfg: SystemConfig | str, target_solver=None, vxc_target=None) 
                     parent_tree=ptree, child_tree=ctree))
 
     # forward solve for the target density
+    if isinstance(target_solver, str) and target_solver == "atoms":
+        set_target_density(prob, rho_atoms(cfg, quad_xyz), rho_atoms(cfg, S.node_xyz))
+        return prob
     v_ks = v_base + interpolate_child_to_parent_quad(prob, vxc_exact)
     if target_solver is None:
         target_solver = dense_ground_state
@@ -396,10 +412,16 @@ def build_problem(cfg: SystemConfig | str, target_solver=None, vxc_target=None) 
 
 def set_target(prob: Problem, psi_nodal: np.ndarray, occ: np.ndarray):
     """rho*, loss weights and adjoint constraints from a forward ground state."""
-    cfg = prob.cfg
     rho_q = density_at_quad(prob, psi_nodal, occ)
+    rho_n = 2.0 * np.sum(np.asarray(occ)[None, :] * psi_nodal ** 2, axis=1)
+    set_target_density(prob, rho_q, rho_n)
+
+
+def set_target_density(prob: Problem, rho_q: np.ndarray, rho_n: np.ndarray):
+    """Install a total target density given at the quad points and the nodes."""
+    cfg = prob.cfg
     prob.rho_target_up = 0.5 * rho_q
-    prob.rho_target_nodal = 2.0 * np.sum(np.asarray(occ)[None, :] * psi_nodal ** 2, axis=1)
+    prob.rho_target_nodal = rho_n
     if cfg.unit_weights:
         prob.weight = np.ones_like(rho_q)
     else:

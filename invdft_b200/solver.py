@@ -1,0 +1,244 @@
+"""Python mirror of the reference's interfaces for the force-evaluation path.
+
+``InverseDFTSolverFunction`` mirrors include/InverseDFTSolverFunction.h:51-384
+(``getForceVector``, ``dotProduct``, ``getInitialGuess``/``setInitialGuess``/
+``setSolution``); ``MultiVectorAdjointLinearSolverProblem`` mirrors
+include/MultiVectorAdjointLinearSolverProblem.h:15-214 (``updateInputPsi``,
+``computeRhs``, ``vmult``, ``precondition_Jacobi``, ``precondition_JacobiSqrt``,
+``distributeX``); ``BFGSInverseDFTSolver`` mirrors BFGSInverseDFTSolver.h:28-119.
+Every call goes through the C ABI of libinvdft_b200.so; device blocks are
+torch CUDA tensors of shape [n_nodes, B], float64.
+Where the reference aborts (AssertThrow), these raise ``InvDFTError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import native
+from .native import InvDFTError, Stats, f64, ptr
+
+
+def _check(lib, ctx, rc):
+    if rc != 0:
+        raise InvDFTError(rc, lib.invdft_last_error(ctx).decode())
+
+
+class InverseDFTSolverFunction:
+    """Force evaluation v_xc -> (dL/dv_xc, L) on one B200."""
+
+    def __init__(self, problem, params: native.Params | None = None, **overrides):
+        self.lib = native.load()
+        self.problem = problem
+        self.params = params or native.default_params(**overrides)
+        keep: list = []
+        desc = native.make_desc(problem, keep)
+        ctx = C.c_void_p()
+        rc = self.lib.invdft_force_create(C.byref(desc), C.byref(self.params), C.byref(ctx))
+        if rc != 0:
+            raise InvDFTError(rc, self.lib.invdft_last_error(None).decode())
+        self.ctx = ctx
+        self.n_child = problem.n_child_nodes
+        self.N = problem.n_states
+        self._pot = None
+        self.last_stats: dict = {}
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.invdft_force_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, **overrides):
+        for k, v in overrides.items():
+            setattr(self.params, k, v)
+        _check(self.lib, self.ctx, self.lib.invdft_set_params(self.ctx, C.byref(self.params)))
+
+    def set_subspace(self, X):
+        X = f64(X)
+        if X.shape != (self.problem.n_nodes, self.N):
+            raise ValueError("subspace shape mismatch")
+        _check(self.lib, self.ctx, self.lib.invdft_set_subspace(self.ctx, ptr(X)))
+
+    # -- reference interface -------------------------------------------------
+    def get_force_vector(self, pot):
+        """Returns (force, loss, stats); ``pot`` (numpy) is distributed then has its
+        constrained entries zeroed in place, as the reference does."""
+        if not isinstance(pot, np.ndarray) or pot.dtype != np.float64 or not pot.flags.c_contiguous:
+            raise TypeError("pot must be a contiguous float64 numpy array")
+        if pot.shape != (self.n_child,):
+            raise ValueError("pot has the wrong length")
+        force = np.zeros(self.n_child)
+        loss = C.c_double()
+        st = Stats()
+        _check(self.lib, self.ctx, self.lib.invdft_force_eval(self.ctx, ptr(pot), ptr(force), C.byref(loss),
+                                                               C.byref(st)))
+        self.last_stats = st.as_dict()
+        return force, float(loss.value), self.last_stats
+
+    def getForceVector(self, pot: list, force: list, loss: list):
+        """getForceVector(pot, force, loss) with per-spin lists (one spin here)."""
+        if len(pot) != 1:
+            raise InvDFTError(5, "one spin channel is supported")
+        f, L, _ = self.get_force_vector(pot[0])
+        force[:] = [f]
+        loss[:] = [L]
+
+    def dotProduct(self, a, b, blockSize: int = 1):
+        if blockSize != 1:
+            a = f64(a).reshape(-1, blockSize)
+            b = f64(b).reshape(-1, blockSize)
+            return list(np.einsum("ij,ij->j", a, b))
+        a, b = f64(a), f64(b)
+        out = C.c_double()
+        _check(self.lib, self.ctx, self.lib.invdft_dot(self.ctx, ptr(a), ptr(b), a.size, C.byref(out)))
+        return [out.value]
+
+    def dot_product(self, a, b) -> float:
+        return self.dotProduct(a, b)[0]
+
+    def getInitialGuess(self):
+        return [self._pot.copy()] if self._pot is not None else None
+
+    def setInitialGuess(self, pot, target_pot_values=None):
+        self._pot = f64(pot[0]).copy()
+
+    def setSolution(self, pot):
+        self._pot = f64(pot[0]).copy()
+
+    # -- results of the last evaluation ---------------------------------------
+    def solve_eigen(self, pot):
+        st = Stats()
+        _check(self.lib, self.ctx, self.lib.invdft_solve_eigen(self.ctx, ptr(pot), C.byref(st)))
+        return st.as_dict()
+
+    def eigen(self):
+        e, o, mu = np.zeros(self.N), np.zeros(self.N), C.c_double()
+        _check(self.lib, self.ctx, self.lib.invdft_get_eigen(self.ctx, ptr(e), ptr(o), C.byref(mu)))
+        return e, o, mu.value
+
+    def psi(self):
+        out = np.zeros((self.problem.n_nodes, self.N))
+        _check(self.lib, self.ctx, self.lib.invdft_get_psi(self.ctx, ptr(out)))
+        return out
+
+    def density(self):
+        out = np.zeros(self.problem.n_cells * self.problem.nq)
+        _check(self.lib, self.ctx, self.lib.invdft_get_density(self.ctx, ptr(out)))
+        return out
+
+    def child_quad_products(self):
+        out = np.zeros(self.problem.n_child_cells * 8)
+        _check(self.lib, self.ctx, self.lib.invdft_get_child_quad_products(self.ctx, ptr(out)))
+        return out
+
+    def set_potential(self, pot):
+        pot = f64(pot).copy()
+        _check(self.lib, self.ctx, self.lib.invdft_set_potential(self.ctx, ptr(pot)))
+
+    def hx(self, x):
+        """Lowdin HX of a torch CUDA float64 block [n_nodes, B]."""
+        import torch
+        x = x.contiguous()
+        y = torch.empty_like(x)
+        _check(self.lib, self.ctx, self.lib.invdft_hx(self.ctx, C.c_void_p(x.data_ptr()),
+                                                       C.c_void_p(y.data_ptr()), x.shape[1]))
+        return y
+
+    def bfgs_solve(self, pot, max_iter: int, tol: float = 1e-12, line_search_iters: int = 1,
+                   line_search_tol: float = 1e-6, history: int = 100):
+        pot = f64(pot).copy()
+        losses = np.zeros(2 * max_iter + 1)
+        n = C.c_int32()
+        _check(self.lib, self.ctx, self.lib.invdft_bfgs_solve(self.ctx, ptr(pot), max_iter, tol,
+                                                               line_search_iters, line_search_tol, history,
+                                                               ptr(losses), C.byref(n)))
+        return pot, losses[:n.value]
+
+
+class MultiVectorAdjointLinearSolverProblem:
+    """The adjoint operator of one block, on torch CUDA float64 tensors."""
+
+    def __init__(self, fn: InverseDFTSolverFunction):
+        self.fn = fn
+        self.lib = fn.lib
+        self.B = 0
+
+    def _c(self, rc):
+        _check(self.lib, self.fn.ctx, rc)
+
+    @staticmethod
+    def _dp(t):
+        import torch
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+            raise TypeError("expected a contiguous float64 CUDA tensor")
+        return C.c_void_p(t.data_ptr())
+
+    def updateInputPsi(self, psi, occupancy, u_vals, degeneracy, fermi_energy, eigenvalues, blockSize):
+        B = int(blockSize)
+        occ = f64(occupancy)
+        eig = f64(eigenvalues)
+        dptr = np.zeros(B + 1, dtype=np.int32)
+        idx = []
+        for i in range(B):
+            idx.extend(int(j) for j in degeneracy[i])
+            dptr[i + 1] = len(idx)
+        didx = np.asarray(idx if idx else [0], dtype=np.int32)
+        self._c(self.lib.invdft_adjoint_update_psi(self.fn.ctx, self._dp(psi), ptr(occ), self._dp(u_vals),
+                                                   ptr(dptr), ptr(didx), float(fermi_energy), ptr(eig), B))
+        self.B = B
+
+    def computeRhs(self, out=None):
+        import torch
+        if out is None:
+            out = torch.empty((self.fn.problem.n_nodes, self.B), dtype=torch.float64, device="cuda")
+        self._c(self.lib.invdft_adjoint_compute_rhs(self.fn.ctx, self._dp(out)))
+        return out
+
+    def vmult(self, Ax, x, blockSize=None):
+        self._c(self.lib.invdft_adjoint_vmult(self.fn.ctx, self._dp(Ax), self._dp(x)))
+
+    def precondition_Jacobi(self, dst, src, omega=0.0):
+        self._c(self.lib.invdft_adjoint_precondition_jacobi(self.fn.ctx, self._dp(dst), self._dp(src), omega))
+
+    def precondition_JacobiSqrt(self, dst, src, omega=0.0):
+        self._c(self.lib.invdft_adjoint_precondition_jacobi_sqrt(self.fn.ctx, self._dp(dst), self._dp(src),
+                                                                 omega))
+
+    def distributeX(self, x):
+        self._c(self.lib.invdft_adjoint_distribute_x(self.fn.ctx, self._dp(x)))
+
+    def solve(self, x, tol: float, max_iter: int):
+        iters = np.zeros(self.B, dtype=np.int32)
+        self._c(self.lib.invdft_adjoint_solve(self.fn.ctx, self._dp(x), tol, max_iter, ptr(iters)))
+        return iters
+
+
+class BFGSInverseDFTSolver:
+    """L-BFGS with the CP line search (BFGSInverseDFTSolver.cpp:467-627), run in C++."""
+
+    def __init__(self, max_iter: int, tol: float = 1e-12, line_search_iters: int = 1,
+                 line_search_tol: float = 1e-6, history: int = 100):
+        self.max_iter, self.tol = max_iter, tol
+        self.ls_iters, self.ls_tol, self.history = line_search_iters, line_search_tol, history
+        self.losses = None
+        self._x = None
+
+    def solve(self, fn: InverseDFTSolverFunction, lsType: str = "CP"):
+        if lsType != "CP":
+            raise InvDFTError(5, "only the CP line search is implemented")
+        x0 = fn.getInitialGuess()
+        if x0 is None:
+            raise InvDFTError(7, "setInitialGuess has not been called")
+        self._x, self.losses = fn.bfgs_solve(x0[0], self.max_iter, self.tol, self.ls_iters, self.ls_tol,
+                                             self.history)
+        return self._x
+
+    def getSolution(self):
+        return [self._x]

@@ -23,7 +23,7 @@ from .fe import (CellOps, child_to_parent_quad, distribute, integrate_child_shap
 @dataclass
 class ForceParams:
     """Knobs of the hot path (inverseDFTParameters / dftParameters names)."""
-    cheb_degree: int = 50                  # CHEBYSHEV POLYNOMIAL DEGREE
+    cheb_degree: int = 50                  # CHEBYSHEV POLYNOMIAL DEGREE (0: from the spectrum bound)
     max_cheb_passes: int = 100             # MAX CHEBYSHEV PASSES
     cheby_tol: float = 1e-6                # CHEBYSHEV FILTER TOLERANCE
     initial_tol_cheb: float = 1e-6         # INITIAL TOL FOR CHEBYSHEV FILTERING
@@ -55,6 +55,18 @@ class ForceStats:
     eigenvalues: np.ndarray | None = None
     occupancy: np.ndarray | None = None
     eta: list = field(default_factory=list)
+    degree: int = 0
+
+
+def auto_degree(upper_bound: float) -> int:
+    """Filter degree when none is given: ceil(3 sqrt(b)) clamped to [24, 500].
+
+    The damping of a state at relative distance d below the unwanted interval
+    [a, b] is cosh(m acosh(1 + 2 d / (b - a))) ~ exp(2 m sqrt(d / b)), so a
+    degree growing like sqrt(b) keeps the per-pass reduction roughly fixed as
+    the mesh is refined (the role of DFT-FE's automatic degree choice)."""
+    import math
+    return int(min(500, max(24, math.ceil(3.0 * math.sqrt(max(upper_bound, 0.0))))))
 
 
 def evaluate_degeneracy_map(eig, tol):
@@ -115,6 +127,8 @@ class InverseDFTSolverFunction:
         self.ops.cell_hamiltonians(self.v_ks)
         hx = self.ops.hx
         lo, b = lanczos_bounds(hx, lanczos_start(prob.n_nodes, self.free), prm.lanczos_steps)
+        degree = prm.cheb_degree if prm.cheb_degree > 0 else auto_degree(b)
+        stats.degree = degree
         stats.passes = 0
         while True:
             if self.eig is None:
@@ -123,7 +137,7 @@ class InverseDFTSolverFunction:
             else:
                 a0 = float(self.eig[0])
                 a = float(self.eig[-1])
-            self.X, self.eig, res = chfsi_pass(hx, self.X, prm.cheb_degree, a, b, a0)
+            self.X, self.eig, res = chfsi_pass(hx, self.X, degree, a, b, a0)
             mu = fermi_energy(self.eig, prob.n_electrons, prob.temperature)
             occ = partial_occupancy(self.eig, mu, prob.temperature)
             homo = 0

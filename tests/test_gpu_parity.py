@@ -1,0 +1,188 @@
+"""GPU parity: the CUDA path (through the C ABI) against the FP64 oracle.
+
+Tolerances are the FP64 bar: eigenvalues within 1e-10 Ha, force within 1e-10
+relative L2, v_xc after a fixed number of BFGS iterations within 1e-7
+relative L2; per-operator checks (HX, rhs, vmult, ...) within 1e-12.
+"""
+import numpy as np
+import pytest
+
+from conftest import native_params, oracle_params, problem, rel
+
+pytestmark = pytest.mark.gpu
+
+TOL_OP = 1e-12
+TOL_FORCE = 1e-10
+TOL_EIG = 1e-10
+
+
+def _pair(name, target=None, **kw):
+    from invdft_b200.solver import InverseDFTSolverFunction
+    from oracle import InverseDFTSolverFunction as Oracle
+    if target == "atoms":
+        from invdft_b200.problem.system import build_problem
+        P = build_problem(name, target_solver="atoms")
+    else:
+        P = problem(name)
+    return P, InverseDFTSolverFunction(P, native_params(**kw)), Oracle(P, oracle_params(**kw))
+
+
+@pytest.mark.parametrize("name,target", [("tiny_h2", None), ("tiny_h2_p4", "atoms"), ("tiny_h2_p5", "atoms")])
+def test_hx_matches_oracle(name, target):
+    import torch
+    P, fn, orc = _pair(name, target)
+    pot = P.vxc_init.copy()
+    fn.set_potential(pot)
+    from oracle.fe import child_to_parent_quad
+    orc.ops.cell_hamiltonians(P.v_base + child_to_parent_quad(P, pot))
+    rng = np.random.default_rng(3)
+    for B in (1, 3, P.n_states):
+        x = rng.standard_normal((P.n_nodes, B))
+        x[~orc.free] = 0.0
+        y = fn.hx(torch.from_numpy(x).cuda()).cpu().numpy()
+        assert rel(y, orc.ops.hx(x)) < TOL_OP
+
+
+@pytest.mark.parametrize("name", ["tiny_h2", "small_lih"])
+def test_eigensolve_and_density(name):
+    P, fn, orc = _pair(name)
+    pot = P.vxc_init.copy()
+    st = fn.solve_eigen(pot.copy())
+    from oracle.force import ForceStats
+    ost = ForceStats()
+    from oracle.fe import distribute
+    orc.solve_eigen(distribute(P.cons_child, pot.copy()), ost)
+    e, o, mu = fn.eigen()
+    assert st["passes"] == ost.passes
+    assert np.max(np.abs(e - orc.eig)) < TOL_EIG
+    assert abs(mu - orc.mu) < 1e-9
+    rho = fn.density()
+    assert rel(rho, orc.density()) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["tiny_h2", "small_lih"])
+def test_force_vector_parity(name):
+    P, fn, orc = _pair(name)
+    for k in range(2):   # second call exercises the warm start and adaptive tolerances
+        pot = P.vxc_init + 0.01 * k * np.sin(P.child_node_xyz[:, 0])
+        pg = pot.copy()
+        f_g, L_g, st = fn.get_force_vector(pg)
+        f_o, L_o, ost = orc.get_force_vector(pot.copy())
+        assert st["passes"] == ost.passes
+        assert abs(L_g - L_o) <= 1e-10 * abs(L_o)
+        assert rel(f_g, f_o) < TOL_FORCE, (rel(f_g, f_o), st, ost.minres_iters)
+        assert np.all(pg[P.cons_child.nodes] == 0.0)
+        assert np.all(f_g[P.cons_child.nodes] == 0.0)
+        assert abs(st["l1_error"] - ost.l1_error) <= 1e-9 * abs(ost.l1_error)
+
+
+def test_force_vector_blocks_and_p4():
+    """Block size below N (degeneracy-aware partition) and a p=4 mesh."""
+    P, fn, orc = _pair("tiny_h2_p4", "atoms", block_size=2)
+    pot = P.vxc_init.copy()
+    f_g, L_g, st = fn.get_force_vector(pot.copy())
+    f_o, L_o, ost = orc.get_force_vector(pot.copy())
+    assert st["n_blocks"] >= 2
+    assert abs(L_g - L_o) <= 1e-10 * abs(L_o)
+    assert rel(f_g, f_o) < TOL_FORCE
+
+
+def test_adjoint_operator_interface():
+    """updateInputPsi / computeRhs / vmult / precondition_* / distributeX through the C ABI."""
+    import torch
+    from invdft_b200.solver import MultiVectorAdjointLinearSolverProblem
+    from oracle.adjoint import AdjointProblem
+    from oracle.force import evaluate_degeneracy_map
+    P, fn, orc = _pair("small_lih")
+    pot = P.vxc_init.copy()
+    fn.get_force_vector(pot.copy())
+    orc.get_force_vector(pot.copy())
+    eig, occ, mu = fn.eigen()
+    psi = fn.psi()
+    rho = fn.density()
+    u = (P.rho_target_up - 0.5 * rho) * P.weight
+    B = P.n_states
+    degen = evaluate_degeneracy_map(list(eig), 0.002)
+    ad = MultiVectorAdjointLinearSolverProblem(fn)
+    dpsi = torch.from_numpy(psi).cuda()
+    du = torch.from_numpy(u).cuda()
+    ad.updateInputPsi(dpsi, occ, du, degen, mu, eig, B)
+    oa = AdjointProblem(orc.ops, P.temperature)
+    oa.update_input_psi(psi, occ, u, degen, mu, eig)
+    rhs = ad.computeRhs().cpu().numpy()
+    assert rel(rhs, oa.compute_rhs()) < TOL_OP
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((P.n_nodes, B))
+    xg = torch.from_numpy(x.copy()).cuda()
+    Ax = torch.empty_like(xg)
+    ad.vmult(Ax, xg)
+    oAx, ox = oa.vmult(x.copy())
+    assert rel(Ax.cpu().numpy(), oAx) < TOL_OP
+    assert rel(xg.cpu().numpy(), ox) < TOL_OP
+    dst = torch.empty_like(xg)
+    ad.precondition_Jacobi(dst, xg)
+    assert rel(dst.cpu().numpy(), oa.precondition_jacobi(ox)) < TOL_OP
+    ad.precondition_JacobiSqrt(dst, xg)
+    assert rel(dst.cpu().numpy(), oa.precondition_jacobi_sqrt(ox)) < TOL_OP
+    xd = torch.from_numpy(x.copy()).cuda()
+    ad.distributeX(xd)
+    assert rel(xd.cpu().numpy(), oa.distribute_x(x.copy())) < 1e-11
+
+
+def test_minres_solution_parity():
+    import torch
+    from invdft_b200.solver import MultiVectorAdjointLinearSolverProblem
+    from oracle.adjoint import AdjointProblem, minres_solve
+    from oracle.force import evaluate_degeneracy_map
+    P, fn, orc = _pair("tiny_h2")
+    pot = P.vxc_init.copy()
+    fn.get_force_vector(pot.copy())
+    eig, occ, mu = fn.eigen()
+    psi = fn.psi()
+    u = (P.rho_target_up - 0.5 * fn.density()) * P.weight
+    B = P.n_states
+    degen = evaluate_degeneracy_map(list(eig), 0.002)
+    ad = MultiVectorAdjointLinearSolverProblem(fn)
+    ad.updateInputPsi(torch.from_numpy(psi).cuda(), occ, torch.from_numpy(u).cuda(), degen, mu, eig, B)
+    x = torch.zeros((P.n_nodes, B), dtype=torch.float64, device="cuda")
+    it_g = ad.solve(x, 1e-10, 500)
+    oa = AdjointProblem(orc.ops, P.temperature)
+    from oracle.fe import child_to_parent_quad, distribute
+    orc.ops.cell_hamiltonians(P.v_base + child_to_parent_quad(P, distribute(P.cons_child, pot.copy())))
+    oa.update_input_psi(psi, occ, u, degen, mu, eig)
+    xo, it_o, _ = minres_solve(oa, 1e-10, 500)
+    xo = oa.distribute_x(xo)
+    assert list(it_g) == list(it_o)
+    assert rel(x.cpu().numpy(), xo) < 1e-10
+
+
+def test_bfgs_trajectory_parity():
+    """v_xc after a fixed number of BFGS iterations within 1e-7 relative L2."""
+    from oracle import BFGSInverseDFTSolver as OBFGS
+    P, fn, orc = _pair("tiny_h2")
+    x0 = P.vxc_init.copy()
+    xg, losses = fn.bfgs_solve(x0.copy(), max_iter=3)
+    ob = OBFGS(max_iter=3)
+    xo, go, Lo = ob.solve(orc, x0.copy())
+    xo = xo.copy()
+    xo[P.cons_child.nodes] = 0.0
+    xg = xg.copy()
+    xg[P.cons_child.nodes] = 0.0
+    assert rel(xg, xo) < 1e-7
+    assert losses[-1] < losses[0]
+
+
+def test_nonfinite_potential_is_reported():
+    from invdft_b200.native import InvDFTError
+    P, fn, _ = _pair("tiny_h2")
+    pot = P.vxc_init.copy()
+    pot[3] = np.nan
+    with pytest.raises(InvDFTError) as ei:
+        fn.get_force_vector(pot)
+    assert ei.value.status == 2
+
+
+def test_minres_iteration_cap_returns_finite():
+    P, fn, _ = _pair("tiny_h2", adjoint_max_iter=1)
+    f, L, st = fn.get_force_vector(P.vxc_init.copy())
+    assert np.all(np.isfinite(f)) and st["minres_iters_max"] <= 1

@@ -1,0 +1,83 @@
+"""Host-side logic on CPU: the L-BFGS mirror, block partitioning, and the
+replica aggregation of bench.py over two gloo ranks."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+class _Quadratic:
+    """L(x) = 1/2 x^T A x - b^T x exposed with the force-evaluation interface."""
+
+    def __init__(self, n=30, seed=0):
+        rng = np.random.default_rng(seed)
+        Q = rng.standard_normal((n, n))
+        self.A = Q @ Q.T / n + np.eye(n)
+        self.b = rng.standard_normal(n)
+        self.calls = 0
+
+    def get_force_vector(self, x):
+        self.calls += 1
+        g = self.A @ x - self.b
+        return g, 0.5 * x @ self.A @ x - self.b @ x, None
+
+    @staticmethod
+    def dot_product(a, b):
+        return float(np.dot(a, b))
+
+
+def test_bfgs_mirror_minimises_a_quadratic():
+    from oracle import BFGSInverseDFTSolver
+    f = _Quadratic()
+    x, g, L = BFGSInverseDFTSolver(max_iter=60, tol=1e-10).solve(f, np.zeros(30))
+    xs = np.linalg.solve(f.A, f.b)
+    assert np.linalg.norm(x - xs) < 1e-6 * np.linalg.norm(xs)
+
+
+def test_block_partition_keeps_degenerate_groups_together():
+    """The block-size shrink rule of InverseDFTSolverFunction.cpp:927-955."""
+    eig = np.array([-1.0, -0.5, -0.4995, -0.2, -0.1999, -0.1998, 0.3])
+    tol, block, N = 0.002, 3, len(eig)
+    blocks, j = [], 0
+    while j < N:
+        bs = min(block, N - j)
+        while j + bs < N and abs(eig[j + bs - 1] - eig[j + bs]) < tol:
+            bs -= 1
+        blocks.append((j, bs))
+        j += bs
+    assert blocks == [(0, 3), (3, 3), (6, 1)]
+
+
+def _replica_worker(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    sys.path.insert(0, ROOT)
+    import bench
+    ms = 100.0 * (rank + 1)
+    v, e2e, tmax = bench.aggregate(ms, ms / 1000.0 * 1.1, steps=4, world=world, dist=dist, device="cpu")
+    out.put((rank, v, e2e, tmax))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_replica_timing_is_max_over_ranks_gloo():
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29500 + (os.getpid() % 1000)
+    procs = [ctx.Process(target=_replica_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, v, e2e, tmax in res:
+        assert tmax == pytest.approx(200.0)
+        assert v == pytest.approx(4 * 2 / 0.2)
+        assert e2e == pytest.approx(4 * 2 / 0.22)

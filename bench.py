@@ -177,6 +177,7 @@ def main():
     ap.add_argument("--config", default="c1_c2h4")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-sample-cells", type=int, default=400)
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample (profiling runs)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -240,11 +241,13 @@ def main():
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record()
         w0 = time.perf_counter()
+        torch.cuda.nvtx.range_push("timed")
         for k in range(args.warmup, total):
             pinned_pot.numpy()[:] = trajectory(P, k, total)
             f, L, st = fn.get_force_vector(pinned_pot.numpy())
             pinned_force.numpy()[:] = f
             stats.append(st)
+        torch.cuda.nvtx.range_pop()
         ev1.record()
         torch.cuda.synchronize()
         t_e2e = time.perf_counter() - w0
@@ -257,8 +260,11 @@ def main():
     per_launch_traffic = _traffic_from_profiles(f"{args.config}:{args.precision}")
     launches = int(sum(s["n_launches"] for s in stats))
     if rank == 0:
-        cpu_v, cpu_meta = cpu_sample(P, int(np.mean([s["n_hx_columns"] for s in stats])), P.n_states,
-                                     args.cpu_sample_cells, threads)
+        if args.no_cpu_baseline:
+            cpu_v, cpu_meta = None, dict(kind="port", cores=threads, sample="skipped (--no-cpu-baseline)")
+        else:
+            cpu_v, cpu_meta = cpu_sample(P, int(np.mean([s["n_hx_columns"] for s in stats])), P.n_states,
+                                         args.cpu_sample_cells, threads)
         line = {
             "metric": METRIC, "value": value, "unit": "force-evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,

@@ -314,7 +314,7 @@ Context::~Context() {
 }
 
 void Context::set_params(const invdft_params *pp) {
-  check(pp->cheb_degree >= 1, "cheb_degree must be >= 1");
+  check(pp->cheb_degree >= 0, "cheb_degree must be >= 0 (0: automatic)");
   check(pp->max_cheb_passes >= 1, "max_cheb_passes must be >= 1");
   check(pp->adjoint_max_iter >= 0, "adjoint_max_iter must be >= 0");
   check(pp->block_size >= 0, "block_size must be >= 0");

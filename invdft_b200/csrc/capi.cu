@@ -191,7 +191,7 @@ invdft_status invdft_hx(invdft_ctx *ctx, const double *d_x, double *d_y, int32_t
   return guard(ctx, [&](invdft::Context &c) {
     if (!d_x || !d_y || B < 1 || B > c.N) throw invdft::StatusError(INVDFT_BAD_ARG, "bad hx arguments");
     c.hx(d_x, d_y, B);
-    INVDFT_CUDA(cudaStreamSynchronize(c.stream));
+    c.check_device_error();
   });
 }
 
@@ -218,7 +218,7 @@ invdft_status invdft_adjoint_compute_rhs(invdft_ctx *ctx, double *d_rhs) {
 invdft_status invdft_adjoint_vmult(invdft_ctx *ctx, double *d_Ax, double *d_x) {
   return guard(ctx, [&](invdft::Context &c) {
     c.adj_vmult(d_Ax, d_x);
-    INVDFT_CUDA(cudaStreamSynchronize(c.stream));
+    c.check_device_error();
   });
 }
 
@@ -250,6 +250,7 @@ invdft_status invdft_adjoint_solve(invdft_ctx *ctx, double *d_x, double tol, int
   return guard(ctx, [&](invdft::Context &c) {
     std::vector<int> its;
     c.adj_minres(d_x, tol, max_iter, its);
+    c.check_device_error();
     if (iters)
       for (size_t i = 0; i < its.size(); ++i) iters[i] = its[i];
   });

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <set>
@@ -114,6 +115,60 @@ void build_scatter(int64_t nrows, int64_t ncell, int per_cell, const int64_t *ce
       }
     }
   }
+}
+
+// Slot layout of cell results (see FeView): direct slots of free nodes sorted by
+// node then by (cell, local); rows of hanging nodes in slots after those,
+// grouped by hanging node (zptr ranges, summed into z[hanging node] first);
+// masters then receive sum_s w_sm z[s] through (hs, hw) lists sorted by
+// master, one entry per (hanging node, master) pair; Dirichlet rows dropped.
+void build_slots(int64_t nrows, int64_t ncell, int per_cell, const int64_t *cell_nodes,
+                 const invdft_constraints &c, std::vector<int> &slot_of, std::vector<int> &dptr,
+                 std::vector<int> &zptr, std::vector<int> &hptr, std::vector<int> &hs,
+                 std::vector<double> &hw) {
+  std::vector<int64_t> crow(nrows, -1), hidx(c.n_rows, -1);
+  for (int64_t r = 0; r < c.n_rows; ++r) crow[c.rows[r]] = r;
+  int64_t nh = 0;
+  for (int64_t r = 0; r < c.n_rows; ++r)
+    if (c.ptr[r + 1] > c.ptr[r]) hidx[r] = nh++;
+  const int64_t tot = ncell * per_cell;
+  if (tot > INT32_MAX) throw StatusError(INVDFT_BAD_ARG, "more than 2^31 cell rows");
+  std::vector<int64_t> cnt(nrows + 1, 0), zcnt(nh + 1, 0), hcnt(nrows + 1, 0);
+  for (int64_t t = 0; t < tot; ++t) {
+    const int64_t n = cell_nodes[t], r = crow[n];
+    if (r < 0) cnt[n + 1]++;
+    else if (hidx[r] >= 0) zcnt[hidx[r] + 1]++;
+  }
+  for (int64_t r = 0; r < c.n_rows; ++r)
+    if (hidx[r] >= 0)
+      for (int64_t k = c.ptr[r]; k < c.ptr[r + 1]; ++k) hcnt[c.masters[k] + 1]++;
+  for (int64_t n = 0; n < nrows; ++n) {
+    cnt[n + 1] += cnt[n];
+    hcnt[n + 1] += hcnt[n];
+  }
+  for (int64_t h = 0; h < nh; ++h) zcnt[h + 1] += zcnt[h];
+  const int64_t ndirect = cnt[nrows];
+  dptr.assign(cnt.begin(), cnt.end());
+  hptr.assign(hcnt.begin(), hcnt.end());
+  zptr.resize(nh + 1);
+  for (int64_t h = 0; h <= nh; ++h) zptr[h] = (int)(ndirect + zcnt[h]);
+  slot_of.assign(tot, -1);
+  std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1), zfill(zcnt.begin(), zcnt.end() - 1);
+  for (int64_t t = 0; t < tot; ++t) {
+    const int64_t n = cell_nodes[t], r = crow[n];
+    if (r < 0) slot_of[t] = (int)fill[n]++;
+    else if (hidx[r] >= 0) slot_of[t] = (int)(ndirect + zfill[hidx[r]]++);
+  }
+  hs.assign(std::max<int64_t>(hcnt[nrows], 1), 0);
+  hw.assign(std::max<int64_t>(hcnt[nrows], 1), 0.0);
+  std::vector<int64_t> hfill(hcnt.begin(), hcnt.end() - 1);
+  for (int64_t r = 0; r < c.n_rows; ++r)
+    if (hidx[r] >= 0)
+      for (int64_t k = c.ptr[r]; k < c.ptr[r + 1]; ++k) {
+        const int64_t m = c.masters[k];
+        hs[hfill[m]] = (int)hidx[r];
+        hw[hfill[m]++] = c.weights[k];
+      }
 }
 
 }  // namespace
@@ -226,9 +281,10 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   const int64_t nmast = d->cons_psi.n_rows ? d->cons_psi.ptr[d->cons_psi.n_rows] : 0;
   std::vector<double> cgw(std::max<int64_t>(nmast, 1), 0.0);
   for (int64_t k = 0; k < nmast; ++k) cgw[k] = d->cons_psi.weights[k] * ism[d->cons_psi.masters[k]];
-  std::vector<int> sp, ssrc;
-  std::vector<double> sw;
-  build_scatter(nn, nc, nd, d->cell_nodes, d->cons_psi, sp, ssrc, sw);
+  std::vector<int> slot_of, dptr_h, zptr_h, hptr_h, hslot_h;
+  std::vector<double> hw_h;
+  build_slots(nn, nc, nd, d->cell_nodes, d->cons_psi, slot_of, dptr_h, zptr_h, hptr_h, hslot_h, hw_h);
+  nhang = (int)zptr_h.size() - 1;
 
   phi.upload(ph, s);
   Kref.upload(K, s);
@@ -245,9 +301,15 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   upload_cons(cadj, d->cons_adj, nn, s);
   upload_cons(cchild, d->cons_child, ncn, s);
   cons_gw.upload(cgw, s);
-  sc_ptr.upload(sp, s);
-  sc_src.upload(ssrc, s);
-  sc_w.upload(sw, s);
+  d_slot_of.upload(slot_of, s);
+  d_dptr.upload(dptr_h, s);
+  d_hptr.upload(hptr_h, s);
+  d_hslot.upload(hslot_h, s);
+  d_zptr.upload(zptr_h, s);
+  d_z.alloc((size_t)std::max(nhang, 1) * 64);
+  d_hw.upload(hw_h, s);
+  d_err.alloc(1);
+  d_err.zero(s);
   sqrtM.upload(sm, s);
   invsqrtM.upload(ism, s);
   diagA.upload(dA, s);
@@ -288,11 +350,21 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   gll.upload(gl, s);
   g2.upload(g2h, 2, s);
 
-  fe.n1 = n1; fe.nd = nd; fe.nq = nq; fe.nc = nc; fe.nnodes = nn;
+  ldh = nd + (nd & 1);
+  fe.n1 = n1; fe.nd = nd; fe.nq = nq; fe.nc = nc; fe.nnodes = nn; fe.ldh = ldh;
   fe.phi = phi.p; fe.cell_h = cell_h.p; fe.cell_nodes = cell_nodes.p; fe.cell_map = cell_map.p;
   fe.cons_ptr = cpsi.ptr.p; fe.cons_masters = cpsi.masters.p; fe.cons_w = cpsi.w.p; fe.cons_gw = cons_gw.p;
   fe.cons_rows = cpsi.rows.p; fe.ncons = cpsi.n;
-  fe.sc_ptr = sc_ptr.p; fe.sc_src = sc_src.p; fe.sc_w = sc_w.p;
+  fe.slot_of = d_slot_of.p; fe.dptr = d_dptr.p; fe.hptr = d_hptr.p; fe.hslot = d_hslot.p; fe.hw = d_hw.p;
+  fe.zptr = d_zptr.p; fe.nhang = nhang; fe.z = d_z.p;
+  fe.err = d_err.p;
+  {
+    // register-blocked row-stream kernel by default; INVDFT_HX_KERNEL=bulk selects
+    // the bulk-asynchronous staged variant
+    const char *v = std::getenv("INVDFT_HX_KERNEL");
+    const std::string k = v ? v : "dmma";
+    hx_variant = k == "bulk" ? 2 : (k == "rowstream" ? 1 : 0);
+  }
   fe.inv_sqrt_mass = invsqrtM.p; fe.sqrt_mass = sqrtM.p;
   cv.ncc = ncc; cv.nchild_nodes = ncn; cv.cell_nodes = ch_nodes.p; cv.jxw = ch_jxw.p; cv.parent = ch_parent.p;
   cv.offset = ch_offset.p; cv.scale = ch_scale.p; cv.pq_child = pq_child.p; cv.pq_xi = pq_xi.p;
@@ -313,6 +385,16 @@ Context::~Context() {
   }
 }
 
+void Context::check_device_error() {
+  int e = 0;
+  INVDFT_CUDA(cudaMemcpyAsync(&e, d_err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  INVDFT_CUDA(cudaStreamSynchronize(stream));
+  if (e) {
+    d_err.zero(stream);
+    throw StatusError(INVDFT_CUDA_ERROR, "a bounded device wait gave up (staged HX kernel)");
+  }
+}
+
 void Context::set_params(const invdft_params *pp) {
   check(pp->cheb_degree >= 0, "cheb_degree must be >= 0 (0: automatic)");
   check(pp->max_cheb_passes >= 1, "max_cheb_passes must be >= 1");
@@ -325,7 +407,7 @@ void Context::set_params(const invdft_params *pp) {
 
 void Context::alloc_state() {
   const int maxB = N;
-  H.alloc((size_t)nc * nd * nd);
+  H.alloc((size_t)nc * ((nd + 1) / 2) * 2 * ldh);
   X.alloc((size_t)nn * N);
   Yb.alloc((size_t)nn * N);
   Zb.alloc((size_t)nn * N);
@@ -370,7 +452,9 @@ void Context::set_subspace(const double *Xh) {
 void Context::cell_gemm(const double *d_x, int Bw) {
   const bool rec = profile && ev_used + 2 <= (int)ev_pool.size();
   if (rec) INVDFT_CUDA(cudaEventRecord(ev_pool[ev_used], stream));
-  launch_hx_cell_gemm(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
+  if (hx_variant == 0) launch_hx_cell_dmma(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
+  else if (hx_variant == 2) launch_hx_cell_gemm_bulk(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
+  else launch_hx_cell_gemm(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
   if (rec) {
     INVDFT_CUDA(cudaEventRecord(ev_pool[ev_used + 1], stream));
     ev_used += 2;
@@ -799,6 +883,10 @@ void Context::adj_minres(double *d_x, double tol, int maxit, std::vector<int> &i
   st.denom = sc + 12 * 64; st.phi = sc + 13 * 64;
   st.active = m_flags.p; st.commit = m_flags.p + 64; st.iters = m_flags.p + 128;
   st.tol = tol;
+  {
+    const size_t need = (size_t)assemble_blocks(fe, Bw) * Bw;
+    if (partial.n < need) partial.alloc(need);
+  }
   launch_minres_init(m_b.p, diagA.p, m_r1.p, m_r2.p, m_y.p, nn, Bw, partial.p, nblocks_red, stream);
   launch_reduce_partials(partial.p, nblocks_red, Bw, st.beta2, stream);
   launch_minres_init_scalars(st, st.beta2, Bw, stream);
@@ -821,8 +909,8 @@ void Context::adj_minres(double *d_x, double tol, int maxit, std::vector<int> &i
     epi.eps = a_eig.p;
     epi.minres_coef = st.coef1;
     epi.dot_partial = partial.p;
-    launch_hx_assemble(fe, Ycell.p, m_yn.p, Bw, epi, nblocks_red, stream);
-    launch_reduce_partials(partial.p, nblocks_red, Bw, st.alfa, stream);
+    const int nparts = launch_hx_assemble(fe, Ycell.p, m_yn.p, Bw, epi, nblocks_red, stream);
+    launch_reduce_partials(partial.p, nparts, Bw, st.alfa, stream);
     n_hx++;
     n_hx_cols += Bw;
     launch_minres_update1(m_r1.p, m_r2.p, m_y.p, m_yn.p, diagA.p, st, nn, Bw, partial.p, nblocks_red, stream);
@@ -973,6 +1061,7 @@ void Context::eval(double *pot, double *force, double *loss, invdft_force_stats 
   ++counter;
   st->n_launches = launch_count() - launches0;
   profile_end(st);
+  check_device_error();
 }
 
 }  // namespace invdft

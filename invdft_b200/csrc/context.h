@@ -43,8 +43,13 @@ class Context {
   DevBuf<int> cell_nodes, cell_map;
   Cons cpsi, cadj, cchild;
   DevBuf<double> cons_gw;
-  DevBuf<int> sc_ptr, sc_src;
-  DevBuf<double> sc_w;
+  DevBuf<int> d_slot_of, d_dptr, d_hptr, d_hslot, d_err, d_zptr;
+  DevBuf<double> d_z;
+  int nhang = 0;
+  DevBuf<double> d_hw;
+  int ldh = 0;
+  int hx_variant = 0;   // 0: FP64 tensor core (mma.sync f64), 1: row-stream DFMA, 2: bulk-staged DFMA
+  void check_device_error();
   DevBuf<double> sqrtM, invsqrtM, diagA, diagSqrtA;
   std::vector<char> h_free;        // unconstrained psi rows
   // child data

@@ -6,6 +6,7 @@
 // column j of H_e with unit stride.
 #include "kernels.cuh"
 
+#include <algorithm>
 #include <atomic>
 
 namespace invdft {
@@ -45,10 +46,67 @@ __device__ void tensor3(const double *A, bool trans, const double *in, double *t
   __syncthreads();
 }
 
+
+// One entry of the cell block X_e (row l, column b) of the gather: the
+// Lowdin-scaled and hanging-distributed value, or the plain nodal value.
+__device__ __forceinline__ double gather_value(const FeView &fe, const double *__restrict__ x, int64_t e, int l,
+                                               int b, int B, int mode) {
+  const int nd = fe.nd;
+  if (mode == GATHER_PLAIN) return x[(int64_t)fe.cell_nodes[e * nd + l] * B + b];
+  const int m = fe.cell_map[e * nd + l];
+  if (m >= 0) return x[(int64_t)m * B + b] * fe.inv_sqrt_mass[m];
+  const int r = -m - 1;
+  double v = 0.0;
+  for (int k = fe.cons_ptr[r]; k < fe.cons_ptr[r + 1]; ++k)
+    v = fma(fe.cons_gw[k], x[(int64_t)fe.cons_masters[k] * B + b], v);
+  return v;
+}
+
+// X_e into shared memory as [rows][ld] (rows >= nd, columns >= B zero), with
+// eight independent load chains in flight per thread.
+__device__ __forceinline__ void gather_cell_block(const FeView &fe, const double *__restrict__ x, int64_t e,
+                                                  int B, int ld, int rows, int mode, double *xs) {
+  constexpr int U = 8;
+  const int total = rows * ld;
+  for (int base = threadIdx.x; base < total; base += blockDim.x * U) {
+    double v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = base + u * blockDim.x;
+      const int l = idx / ld, b = idx - l * ld;
+      v[u] = (idx < total && b < B && l < fe.nd) ? gather_value(fe, x, e, l, b, B, mode) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = base + u * blockDim.x;
+      if (idx < total) xs[idx] = v[u];
+    }
+  }
+}
+
+// dst[0..n) = src[0..n) with eight loads in flight per thread
+template <typename T>
+__device__ __forceinline__ void stage_copy(T *dst, const T *__restrict__ src, int n) {
+  constexpr int U = 8;
+  for (int base = threadIdx.x; base < n; base += blockDim.x * U) {
+    T v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = base + u * blockDim.x;
+      v[u] = i < n ? src[i] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int i = base + u * blockDim.x;
+      if (i < n) dst[i] = v[u];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Cell Hamiltonian H_e = 1/2 h K_ref + N^T diag(v JxW) N by sum factorisation.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(NT) build_cell_h_kernel(int n1, const double *__restrict__ phi,
+__global__ void __launch_bounds__(NT) build_cell_h_kernel(int n1, int ldh, const double *__restrict__ phi,
                                                           const double *__restrict__ vks,
                                                           const double *__restrict__ jxw,
                                                           const double *__restrict__ Kref,
@@ -82,7 +140,7 @@ __global__ void __launch_bounds__(NT) build_cell_h_kernel(int n1, const double *
   }
   __syncthreads();
   const double hh = 0.5 * cell_h[e];
-  double *He = H + e * (int64_t)nd * nd;
+  double *He = H + e * (int64_t)((nd + 1) >> 1) * 2 * ldh;
   for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) {
     const int j = t / nd, i = t % nd;
     const int a = i % n1, b = (i / n1) % n1, c = i / n2;
@@ -90,26 +148,34 @@ __global__ void __launch_bounds__(NT) build_cell_h_kernel(int n1, const double *
     const int aa = a * n1 + ap, bb = b * n1 + bp, cc = c * n1 + cp;
     double s = 0.0;
     for (int q1 = 0; q1 < n1; ++q1) s = fma(P[aa * n1 + q1], T2[(q1 * n2 + bb) * n2 + cc], s);
-    He[t] = fma(hh, Kref[t], s);
+    He[(int64_t)(j >> 1) * 2 * ldh + 2 * i + (j & 1)] = fma(hh, Kref[t], s);
   }
+  // zero the padding row (i = nd) and, for odd nd, the padding column (j = nd)
+  if (ldh > nd)
+    for (int j = threadIdx.x; j < nd; j += blockDim.x) He[(int64_t)(j >> 1) * 2 * ldh + 2 * nd + (j & 1)] = 0.0;
+  if (nd & 1)
+    for (int i = threadIdx.x; i < ldh; i += blockDim.x) He[(int64_t)(nd >> 1) * 2 * ldh + 2 * i + 1] = 0.0;
 }
 
 // ---------------------------------------------------------------------------
 // HX, part 1: Y_e = H_e X_e with the constrained gather fused in.
 // One CTA per cell; thread i owns row i and BC accumulators.
 // ---------------------------------------------------------------------------
-template <int BC>
+template <int BC, int R>
 __global__ void __launch_bounds__(NT) hx_cell_gemm_kernel(FeView fe, const double *__restrict__ H,
                                                           const double *__restrict__ x,
-                                                          double *__restrict__ Ycell, int B,
-                                                          int mode) {
-  extern __shared__ double xs[];  // [nd][BC]
+                                                          double *__restrict__ Ycell, int B, int mode) {
+  // Thread t owns rows R*t .. R*t+R-1 of H_e (register blocking: every vector
+  // value read from shared memory feeds R*2 FMAs per column pair) and streams
+  // them as 16-byte column-pair loads, R*16 contiguous bytes per thread.
+  extern __shared__ double xs[];  // [2*ncp][BC], rows beyond nd zero
   const int nd = fe.nd;
+  const int ncp = (nd + 1) >> 1;
   const int64_t e = blockIdx.x;
-  for (int idx = threadIdx.x; idx < nd * BC; idx += blockDim.x) {
+  for (int idx = threadIdx.x; idx < 2 * ncp * BC; idx += blockDim.x) {
     const int l = idx / BC, b = idx - l * BC;
     double v = 0.0;
-    if (b < B) {
+    if (b < B && l < nd) {
       if (mode == GATHER_PLAIN) {
         const int m = fe.cell_nodes[e * nd + l];
         v = x[(int64_t)m * B + b];
@@ -127,33 +193,269 @@ __global__ void __launch_bounds__(NT) hx_cell_gemm_kernel(FeView fe, const doubl
     xs[idx] = v;
   }
   __syncthreads();
-  const int i = threadIdx.x;
-  double acc[BC];
+  const int r0 = R * threadIdx.x;
+  if (r0 >= nd) return;
+  double acc[R][BC];
 #pragma unroll
-  for (int b = 0; b < BC; ++b) acc[b] = 0.0;
-  if (i < nd) {
-    const double *Hc = H + e * (int64_t)nd * nd + i;
-#pragma unroll 4
-    for (int j = 0; j < nd; ++j) {
-      const double h = __ldcs(Hc + (int64_t)j * nd);
-      const double *xr = xs + j * BC;
+  for (int r = 0; r < R; ++r)
 #pragma unroll
-      for (int b = 0; b < BC; b += 2) {
-        const double2 xv = *reinterpret_cast<const double2 *>(xr + b);
-        acc[b] = fma(h, xv.x, acc[b]);
-        acc[b + 1] = fma(h, xv.y, acc[b + 1]);
+    for (int b = 0; b < BC; ++b) acc[r][b] = 0.0;
+  // rows r0..r0+R-1 are < ldh (ldh >= nd rounded up to even, R divides the
+  // padded row count handled below), so the loads stay inside the cell block
+  const double2 *Hc = reinterpret_cast<const double2 *>(H + e * (int64_t)ncp * 2 * fe.ldh) + r0;
+#pragma unroll 2
+  for (int jp = 0; jp < ncp; ++jp) {
+    double2 h[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) h[r] = (r0 + r < fe.ldh) ? __ldcs(Hc + (int64_t)jp * fe.ldh + r) : make_double2(0.0, 0.0);
+    const double *xr = xs + 2 * jp * BC;
+#pragma unroll
+    for (int b = 0; b < BC; b += 2) {
+      const double2 x0 = *reinterpret_cast<const double2 *>(xr + b);
+      const double2 x1 = *reinterpret_cast<const double2 *>(xr + BC + b);
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        acc[r][b] = fma(h[r].x, x0.x, acc[r][b]);
+        acc[r][b + 1] = fma(h[r].x, x0.y, acc[r][b + 1]);
+        acc[r][b] = fma(h[r].y, x1.x, acc[r][b]);
+        acc[r][b + 1] = fma(h[r].y, x1.y, acc[r][b + 1]);
       }
     }
   }
-  __syncthreads();
-  if (i < nd) {
 #pragma unroll
-    for (int b = 0; b < BC; ++b)
-      if (b < B) xs[i * B + b] = acc[b];
+  for (int r = 0; r < R; ++r) {
+    const int i = r0 + r;
+    if (i < nd) {
+      const int sl = fe.slot_of[e * nd + i];
+      if (sl >= 0) {
+        double *yo = Ycell + (int64_t)sl * B;
+#pragma unroll
+        for (int b = 0; b < BC; ++b)
+          if (b < B) yo[b] = acc[r][b];
+      }
+    }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// HX, part 1, FP64 tensor-core variant: Y_e = H_e X_e with mma.sync m8n8k4 f64
+// (the FP64 tensor path of sm_100a; tcgen05 has no f64 kind).  One CTA per
+// cell, warp w owns 8-row tiles m = w, w+nwarps, ...; for every k-step of 4
+// columns each thread loads one double of H_e (a warp reads two contiguous
+// 128-byte column-pair segments) and one double of X_e from shared memory.
+// ---------------------------------------------------------------------------
+template <int NTILE>
+__global__ void __launch_bounds__(NT) hx_cell_dmma_kernel(FeView fe, const double *__restrict__ H,
+                                                          const double *__restrict__ x,
+                                                          double *__restrict__ Ycell, int B, int mode) {
+  extern __shared__ double xs[];  // [kpad][BP] with BP = 8*NTILE, zero padded
+  constexpr int BP = 8 * NTILE;
+  const int nd = fe.nd, ldh = fe.ldh;
+  const int ncol = 2 * ((nd + 1) >> 1);          // stored columns (pair layout)
+  const int ksteps = (nd + 3) >> 2;
+  const int kpad = 4 * ksteps;
+  const int64_t e = blockIdx.x;
+  gather_cell_block(fe, x, e, B, BP, kpad, mode, xs);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const double *He = H + e * (int64_t)(ncol >> 1) * 2 * ldh;
+  const int mtiles = (nd + 7) >> 3;
+  for (int mt = warp; mt < mtiles; mt += nwarps) {
+    const int row = 8 * mt + g;
+    const bool row_ok = row < ldh;
+    double c[NTILE][2];
+#pragma unroll
+    for (int n = 0; n < NTILE; ++n) c[n][0] = c[n][1] = 0.0;
+    // two-stage register pipeline: the next U k-steps of H are in flight while
+    // the current U feed the tensor core
+    constexpr int U = 8;
+    auto load_a = [&](int ks) -> double {
+      const int k = 4 * ks + t;
+      return (row_ok && ks < ksteps && k < ncol) ? __ldcs(He + (int64_t)(k >> 1) * 2 * ldh + 2 * row + (k & 1)) : 0.0;
+    };
+    double a0[U], a1[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) a0[u] = load_a(u);
+    for (int ks0 = 0; ks0 < ksteps; ks0 += U) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) a1[u] = load_a(ks0 + U + u);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = 4 * (ks0 + u) + t;
+        if (ks0 + u < ksteps) {
+#pragma unroll
+          for (int n = 0; n < NTILE; ++n) {
+            const double bv = xs[k * BP + 8 * n + g];   // B[t][g] = X_e[k][8n+g]
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                         : "+d"(c[n][0]), "+d"(c[n][1])
+                         : "d"(a0[u]), "d"(bv));
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) a0[u] = a1[u];
+    }
+    if (row < nd) {
+      const int sl = fe.slot_of[e * nd + row];
+      if (sl >= 0) {
+        double *yo = Ycell + (int64_t)sl * B;
+#pragma unroll
+        for (int n = 0; n < NTILE; ++n) {
+          const int col = 8 * n + 2 * t;
+          if (col < B) yo[col] = c[n][0];
+          if (col + 1 < B) yo[col + 1] = c[n][1];
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// HX, part 1, bulk-asynchronous variant.  Persistent CTAs walk their cells;
+// thread 0 streams contiguous column panels of H_e (PW columns x ldh doubles)
+// with cp.async.bulk into an S-stage shared-memory ring completed through
+// mbarriers, S-1 panels ahead of the consumers.  Every wait is bounded: a wait
+// that gives up sets fe.err and the CTA stops computing (it never hangs).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+constexpr long long kWaitLimit = 1ll << 22;
+
+template <int BC>
+__global__ void __launch_bounds__(NT, 1) hx_gemm_bulk_kernel(FeView fe, const double *__restrict__ H,
+                                                             const double *__restrict__ x,
+                                                             double *__restrict__ Yslot, int B, int mode,
+                                                             int S, int PW) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  const int nd = fe.nd, ldh = fe.ldh;
+  const int np = (nd + PW - 1) / PW;
+  double *stages = reinterpret_cast<double *>(smraw);
+  double *xs = stages + (size_t)S * PW * ldh;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(xs + (size_t)(nd + 1) * BC);
+  const int tid = threadIdx.x;
+  if (blockIdx.x >= fe.nc) return;
+  const int64_t ncell = (fe.nc - 1 - blockIdx.x) / gridDim.x + 1;
+  const int64_t total = ncell * np;
+  if (tid == 0) {
+    for (int st = 0; st < S; ++st) mbar_init(&bars[st], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  double *yo = Ycell + e * (int64_t)nd * B;
-  for (int idx = threadIdx.x; idx < nd * B; idx += blockDim.x) yo[idx] = xs[idx];
+  auto issue = [&](int64_t sq) {
+    const int64_t t = sq / np;
+    const int k = (int)(sq - t * np);
+    const int64_t e = blockIdx.x + t * gridDim.x;
+    const int c0 = k * PW;
+    const int ncol = min(PW, 2 * ((nd + 1) >> 1) - c0);   // even: whole column pairs
+    const uint32_t bytes = (uint32_t)ncol * ldh * 8u;
+    uint64_t *bar = &bars[sq % S];
+    mbar_expect_tx(bar, bytes);
+    bulk_g2s(stages + (sq % S) * (int64_t)PW * ldh,
+             H + e * (int64_t)((nd + 1) >> 1) * 2 * ldh + (int64_t)c0 * ldh, bytes, bar);
+  };
+  if (tid == 0)
+    for (int64_t sq = 0; sq < min((int64_t)S, total); ++sq) issue(sq);
+  bool ok = true;
+  const int i = tid;
+  for (int64_t t = 0; t < ncell; ++t) {
+    const int64_t e = blockIdx.x + t * gridDim.x;
+    for (int idx = tid; idx < (nd + 1) * BC; idx += blockDim.x) {
+      const int l = idx / BC, b = idx - l * BC;
+      double v = 0.0;
+      if (b < B && l < nd) {
+        if (mode == GATHER_PLAIN) {
+          v = x[(int64_t)fe.cell_nodes[e * nd + l] * B + b];
+        } else {
+          const int m = fe.cell_map[e * nd + l];
+          if (m >= 0) {
+            v = x[(int64_t)m * B + b] * fe.inv_sqrt_mass[m];
+          } else {
+            const int r = -m - 1;
+            for (int k = fe.cons_ptr[r]; k < fe.cons_ptr[r + 1]; ++k)
+              v = fma(fe.cons_gw[k], x[(int64_t)fe.cons_masters[k] * B + b], v);
+          }
+        }
+      }
+      xs[idx] = v;
+    }
+    __syncthreads();
+    double acc[BC];
+#pragma unroll
+    for (int b = 0; b < BC; ++b) acc[b] = 0.0;
+    for (int k = 0; k < np; ++k) {
+      const int64_t sq = t * np + k;
+      const int st = (int)(sq % S);
+      const uint32_t par = (uint32_t)((sq / S) & 1);
+      if (ok) {
+        long long it = 0;
+        while (!mbar_try_wait(&bars[st], par)) {
+          if (++it > kWaitLimit) {
+            ok = false;
+            atomicExch(fe.err, 1);
+            break;
+          }
+        }
+      }
+      const int c0 = k * PW;
+      const int ncol = min(PW, 2 * ((nd + 1) >> 1) - c0);
+      if (ok && i < nd) {
+        const double2 *Hs = reinterpret_cast<const double2 *>(stages + (int64_t)st * PW * ldh) + i;
+        const double *xr = xs + (int64_t)c0 * BC;
+        for (int cp = 0; cp < (ncol + 1) / 2; ++cp) {
+          const double2 h = Hs[cp * ldh];
+#pragma unroll
+          for (int b = 0; b < BC; b += 2) {
+            const double2 x0 = *reinterpret_cast<const double2 *>(xr + 2 * cp * BC + b);
+            const double2 x1 = *reinterpret_cast<const double2 *>(xr + (2 * cp + 1) * BC + b);
+            acc[b] = fma(h.x, x0.x, acc[b]);
+            acc[b + 1] = fma(h.x, x0.y, acc[b + 1]);
+            acc[b] = fma(h.y, x1.x, acc[b]);
+            acc[b + 1] = fma(h.y, x1.y, acc[b + 1]);
+          }
+        }
+      }
+      __syncthreads();
+      if (tid == 0 && ok && sq + S < total) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue(sq + S);
+      }
+    }
+    if (ok && i < nd) {
+      const int sl = fe.slot_of[e * nd + i];
+      if (sl >= 0) {
+        double *yo = Yslot + (int64_t)sl * B;
+#pragma unroll
+        for (int b = 0; b < BC; ++b)
+          if (b < B) yo[b] = acc[b];
+      }
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -172,8 +474,11 @@ __global__ void __launch_bounds__(NT) hx_assemble_kernel(FeView fe, const double
   if (rr < RR) {
     for (int64_t n = r0 + rr; n < r1; n += RR) {
       double acc = 0.0;
-      for (int k = fe.sc_ptr[n]; k < fe.sc_ptr[n + 1]; ++k)
-        acc = fma(fe.sc_w[k], Ycell[(int64_t)fe.sc_src[k] * B + j], acc);
+      const int d0 = fe.dptr[n], d1 = fe.dptr[n + 1];
+      // contiguous slots of this node: independent, coalesced loads
+      for (int sl = d0; sl < d1; ++sl) acc += Ycell[(int64_t)sl * B + j];
+      for (int k = fe.hptr[n]; k < fe.hptr[n + 1]; ++k)
+        acc = fma(fe.hw[k], fe.z[(int64_t)fe.hslot[k] * B + j], acc);
       acc *= fe.inv_sqrt_mass[n];
       const int64_t idx = n * B + j;
       switch (epi.kind) {
@@ -187,7 +492,7 @@ __global__ void __launch_bounds__(NT) hx_assemble_kernel(FeView fe, const double
         case AsmEpilogue::VMULT: out[idx] = acc - epi.eps[j] * epi.in[idx]; break;
         case AsmEpilogue::RHS: {
           double v = 0.0;
-          if (fe.sc_ptr[n + 1] > fe.sc_ptr[n] && fe.inv_sqrt_mass[n] != 0.0) {
+          if (d1 > d0 && fe.inv_sqrt_mass[n] != 0.0) {
             double mu = 0.0;
             for (int k = 0; k < B; ++k) mu = fma(epi.Mu[k * B + j], epi.psi[n * B + k], mu);
             v = epi.occ4[j] * acc - 2.0 * fe.sqrt_mass[n] * mu;
@@ -214,6 +519,135 @@ __global__ void __launch_bounds__(NT) hx_assemble_kernel(FeView fe, const double
       epi.dot_partial[(int64_t)blockIdx.x * B + threadIdx.x] = s;
     }
   }
+}
+
+
+// ---------------------------------------------------------------------------
+// HX, part 2 (tiled): a CTA owns TR consecutive nodes, whose direct slots form
+// one contiguous segment [dptr[r0], dptr[r0+TR]).  The segment is streamed
+// into shared memory with coalesced loads and the per-node sums are taken from
+// there; hanging-node contributions (a minority) are read directly.  Thread
+// (rr, j) handles column j of nodes r0+rr, r0+rr+RR, ... (fixed order), so
+// the MINRES dot partials are deterministic.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) hx_assemble_tile_kernel(FeView fe, const double *__restrict__ Ycell,
+                                                              double *__restrict__ out, int B, AsmEpilogue epi,
+                                                              int TR, int cap_slots) {
+  // shared layout: seg [cap][B] | hv [cap][B] | s_in [TR][B] | s_prev [TR][B] | ism [TR] | dp [TR+1] | hp [TR+1]
+  extern __shared__ double sm_asm[];
+  double *seg = sm_asm;
+  double *hv = seg + (size_t)cap_slots * B;
+  double *s_in = hv + (size_t)cap_slots * B;
+  double *s_prev = s_in + (size_t)TR * B;
+  double *ism = s_prev + (size_t)TR * B;
+  int *dp = reinterpret_cast<int *>(ism + TR);
+  int *hp = dp + TR + 1;
+  __shared__ double red[NT];
+  const int64_t r0 = (int64_t)blockIdx.x * TR;
+  const int rows = (int)min((int64_t)TR, fe.nnodes - r0);
+  const bool need_in = epi.kind == AsmEpilogue::CHEB || epi.kind == AsmEpilogue::VMULT ||
+                       epi.kind == AsmEpilogue::MINRES;
+  const bool need_prev = (epi.kind == AsmEpilogue::CHEB && epi.prev) || epi.kind == AsmEpilogue::MINRES;
+  // phase A: independent coalesced loads of everything the tile reads
+  stage_copy(dp, fe.dptr + r0, rows + 1);
+  stage_copy(hp, fe.hptr + r0, rows + 1);
+  stage_copy(ism, fe.inv_sqrt_mass + r0, rows);
+  if (need_in) stage_copy(s_in, epi.in + r0 * B, rows * B);
+  if (need_prev) stage_copy(s_prev, epi.prev + r0 * B, rows * B);
+  __syncthreads();
+  const int s0 = dp[0], s1 = dp[rows];
+  const bool staged = (s1 - s0) <= cap_slots;
+  if (staged) stage_copy(seg, Ycell + (int64_t)s0 * B, (s1 - s0) * B);
+  // weighted rows of the hanging nodes feeding this tile's masters, all
+  // loaded in one wave (z is small and L2-resident)
+  const int h0 = hp[0], h1 = hp[rows];
+  const bool hstaged = (h1 - h0) <= cap_slots;
+  if (hstaged) {
+    constexpr int U = 8;
+    const int n = (h1 - h0) * B;
+    for (int base = threadIdx.x; base < n; base += blockDim.x * U) {
+      double v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int i = base + u * blockDim.x;
+        const int k = h0 + i / B;
+        v[u] = i < n ? fe.hw[k] * fe.z[(int64_t)fe.hslot[k] * B + i % B] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int i = base + u * blockDim.x;
+        if (i < n) hv[i] = v[u];
+      }
+    }
+  }
+  __syncthreads();
+  const int RR = NT / B;
+  const int j = threadIdx.x % B, rr = threadIdx.x / B;
+  double dot = 0.0;
+  if (rr < RR) {
+    for (int lr = rr; lr < rows; lr += RR) {
+      const int64_t n = r0 + lr;
+      const int d0 = dp[lr], d1 = dp[lr + 1];
+      double acc = 0.0;
+      if (staged)
+        for (int sl = d0; sl < d1; ++sl) acc += seg[(sl - s0) * B + j];
+      else
+        for (int sl = d0; sl < d1; ++sl) acc += Ycell[(int64_t)sl * B + j];
+      if (hstaged)
+        for (int k = hp[lr]; k < hp[lr + 1]; ++k) acc += hv[(k - h0) * B + j];
+      else
+        for (int k = hp[lr]; k < hp[lr + 1]; ++k) acc = fma(fe.hw[k], fe.z[(int64_t)fe.hslot[k] * B + j], acc);
+      acc *= ism[lr];
+      const int64_t idx = n * B + j;
+      const int li = lr * B + j;
+      switch (epi.kind) {
+        case AsmEpilogue::STORE: out[idx] = acc; break;
+        case AsmEpilogue::CHEB: {
+          double v = epi.alpha * (acc - epi.c * s_in[li]);
+          if (epi.prev) v -= epi.beta * s_prev[li];
+          out[idx] = v;
+          break;
+        }
+        case AsmEpilogue::VMULT: out[idx] = acc - epi.eps[j] * s_in[li]; break;
+        case AsmEpilogue::RHS: {
+          double v = 0.0;
+          if (d1 > d0 && ism[lr] != 0.0) {
+            double mu = 0.0;
+            for (int k = 0; k < B; ++k) mu = fma(epi.Mu[k * B + j], epi.psi[n * B + k], mu);
+            v = epi.occ4[j] * acc - 2.0 * fe.sqrt_mass[n] * mu;
+          }
+          out[idx] = v;
+          break;
+        }
+        case AsmEpilogue::MINRES: {
+          const double vv = s_in[li];
+          const double yn = acc - epi.eps[j] * vv - epi.minres_coef[j] * s_prev[li];
+          out[idx] = yn;
+          dot = fma(vv, yn, dot);
+          break;
+        }
+      }
+    }
+  }
+  if (epi.kind == AsmEpilogue::MINRES) {
+    red[threadIdx.x] = dot;
+    __syncthreads();
+    if (threadIdx.x < B) {
+      double sum = 0.0;
+      for (int q = 0; q < RR; ++q) sum += red[q * B + threadIdx.x];
+      epi.dot_partial[(int64_t)blockIdx.x * B + threadIdx.x] = sum;
+    }
+  }
+}
+
+// z[h][j] = sum of the cell rows of hanging node h (contiguous slots)
+__global__ void hanging_sum_kernel(FeView fe, const double *__restrict__ Ycell, int B) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)fe.nhang * B) return;
+  const int h = (int)(idx / B), j = (int)(idx % B);
+  double acc = 0.0;
+  for (int sl = fe.zptr[h]; sl < fe.zptr[h + 1]; ++sl) acc += Ycell[(int64_t)sl * B + j];
+  fe.z[idx] = acc;
 }
 
 __global__ void scale_rows_kernel(const double *d, const double *x, double *y, int64_t n, int B) {
@@ -276,12 +710,16 @@ __global__ void __launch_bounds__(NT) gram_kernel(const double *__restrict__ A, 
   }
 }
 
-__global__ void reduce_partials_kernel(const double *partial, int nparts, int width, double *out) {
-  const int o = blockIdx.x * blockDim.x + threadIdx.x;
-  if (o >= width) return;
+// out[o] = sum_g partial[g*width + o]; one CTA per output, fixed summation
+// order (strided thread sums, then a fixed tree), so results are reproducible.
+__global__ void __launch_bounds__(NT) reduce_partials_kernel(const double *partial, int nparts, int width,
+                                                             double *out) {
+  __shared__ double red[32];
+  const int o = blockIdx.x;
   double s = 0.0;
-  for (int g = 0; g < nparts; ++g) s += partial[(int64_t)g * width + o];
-  out[o] = s;
+  for (int g = threadIdx.x; g < nparts; g += blockDim.x) s += partial[(int64_t)g * width + o];
+  s = block_sum<NT>(s, red);
+  if (threadIdx.x == 0) out[o] = s;
 }
 
 __global__ void __launch_bounds__(NT) rotate_kernel(const double *__restrict__ Y, const double *__restrict__ T,
@@ -408,7 +846,8 @@ __global__ void __launch_bounds__(NT) r_cell_kernel(FeView fe, const double *__r
     tensor3(A, true, b1, b0, b2, n1, CH);
     for (int idx = threadIdx.x; idx < nd * CH; idx += blockDim.x) {
       const int l = idx / CH, k = idx % CH;
-      if (k < w) Ycell[(e * nd + l) * B + c0 + k] = b0[idx];
+      const int sl = fe.slot_of[e * nd + l];
+      if (k < w && sl >= 0) Ycell[(int64_t)sl * B + c0 + k] = b0[idx];
     }
   }
 }
@@ -808,44 +1247,138 @@ void launch_build_cell_h(const FeView &fe, const double *vks, const double *jxw,
     INVDFT_CUDA(cudaFuncSetAttribute(build_cell_h_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     attr = true;
   }
-  build_cell_h_kernel<<<(unsigned)fe.nc, NT, smem, s>>>(n1, fe.phi, vks, jxw, Kref, fe.cell_h, H);
+  build_cell_h_kernel<<<(unsigned)fe.nc, NT, smem, s>>>(n1, fe.ldh, fe.phi, vks, jxw, Kref, fe.cell_h, H);
   INVDFT_LAUNCH_CHECK();
 }
 
-template <int BC>
+template <int BC, int R>
 static void hx_gemm_bc(const FeView &fe, const double *H, const double *x, double *Ycell, int B, int mode,
                        cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
-    INVDFT_CUDA(cudaFuncSetAttribute(hx_cell_gemm_kernel<BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_cell_gemm_kernel<BC, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      200 * 1024));
     attr = true;
   }
-  const int threads = ((fe.nd + 31) / 32) * 32;
+  const int rows = (fe.nd + R - 1) / R;
+  const int threads = ((rows + 31) / 32) * 32;
   if (threads > NT) throw StatusError(5, "cell too large for the FP64 HX kernel");
-  const size_t smem = sizeof(double) * (size_t)fe.nd * BC;
-  hx_cell_gemm_kernel<BC><<<(unsigned)fe.nc, threads, smem, s>>>(fe, H, x, Ycell, B, mode);
+  const size_t smem = sizeof(double) * (size_t)(fe.nd + 1) * BC;
+  hx_cell_gemm_kernel<BC, R><<<(unsigned)fe.nc, threads, smem, s>>>(fe, H, x, Ycell, B, mode);
   INVDFT_LAUNCH_CHECK();
 }
 
 void launch_hx_cell_gemm(const FeView &fe, const double *H, const double *x, double *Ycell, int B,
                          int gather_mode, cudaStream_t s) {
-  if (B <= 2) hx_gemm_bc<2>(fe, H, x, Ycell, B, gather_mode, s);
-  else if (B <= 4) hx_gemm_bc<4>(fe, H, x, Ycell, B, gather_mode, s);
-  else if (B <= 8) hx_gemm_bc<8>(fe, H, x, Ycell, B, gather_mode, s);
-  else if (B <= 16) hx_gemm_bc<16>(fe, H, x, Ycell, B, gather_mode, s);
-  else if (B <= 32) hx_gemm_bc<32>(fe, H, x, Ycell, B, gather_mode, s);
-  else if (B <= 64) hx_gemm_bc<64>(fe, H, x, Ycell, B, gather_mode, s);
+  if (B <= 2) hx_gemm_bc<2, 1>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 4) hx_gemm_bc<4, 1>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 8) hx_gemm_bc<8, 1>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 16) hx_gemm_bc<16, 1>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 32) hx_gemm_bc<32, 1>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 64) hx_gemm_bc<64, 1>(fe, H, x, Ycell, B, gather_mode, s);
   else throw StatusError(5, "block width above 64");
 }
 
-void launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B, const AsmEpilogue &epi,
-                        int dot_blocks, cudaStream_t s) {
-  if (B > NT) throw StatusError(5, "block width above 256");
-  const int nb = dot_blocks > 0 ? dot_blocks : pick_blocks(fe.nnodes, 64);
-  const int64_t rpb = (fe.nnodes + nb - 1) / nb;
-  hx_assemble_kernel<<<nb, NT, 0, s>>>(fe, Ycell, out, B, epi, rpb);
+
+template <int NTILE>
+static void hx_dmma_nt(const FeView &fe, const double *H, const double *x, double *Ycell, int B, int mode,
+                       cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_cell_dmma_kernel<NTILE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     200 * 1024));
+    attr = true;
+  }
+  const int mtiles = (fe.nd + 7) / 8;
+  const int threads = std::min(NT, 32 * std::max(1, std::min(8, mtiles)));
+  const int kpad = 4 * ((fe.nd + 3) / 4);
+  const size_t smem = sizeof(double) * (size_t)kpad * 8 * NTILE;
+  hx_cell_dmma_kernel<NTILE><<<(unsigned)fe.nc, threads, smem, s>>>(fe, H, x, Ycell, B, mode);
   INVDFT_LAUNCH_CHECK();
+}
+
+void launch_hx_cell_dmma(const FeView &fe, const double *H, const double *x, double *Ycell, int B,
+                         int gather_mode, cudaStream_t s) {
+  if (B <= 8) hx_dmma_nt<1>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 16) hx_dmma_nt<2>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 24) hx_dmma_nt<3>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 32) hx_dmma_nt<4>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 48) hx_dmma_nt<6>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 64) hx_dmma_nt<8>(fe, H, x, Ycell, B, gather_mode, s);
+  else throw StatusError(5, "block width above 64");
+}
+
+template <int BC>
+static void hx_gemm_bulk_bc(const FeView &fe, const double *H, const double *x, double *Yslot, int B, int mode,
+                            cudaStream_t s) {
+  static bool attr = false;
+  static int nsm = 0;
+  if (!attr) {
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_gemm_bulk_kernel<BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     210 * 1024));
+    int dev = 0;
+    INVDFT_CUDA(cudaGetDevice(&dev));
+    INVDFT_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    attr = true;
+  }
+  const int threads = ((fe.nd + 31) / 32) * 32;
+  if (threads > NT) throw StatusError(5, "cell too large for the FP64 HX kernel");
+  const int PW = 16;
+  const size_t stage = (size_t)PW * fe.ldh * 8;
+  const size_t xsb = (size_t)(fe.nd + 1) * BC * 8;
+  const size_t budget = 200 * 1024;
+  if (xsb + 2 * stage + 64 > budget) throw StatusError(5, "block too wide for the staged HX kernel");
+  int S = (int)((budget - xsb - 64) / stage);
+  if (S > 8) S = 8;
+  const size_t smem = (size_t)S * stage + xsb + (size_t)S * 8;
+  const int grid = (int)std::min<int64_t>(fe.nc, nsm);
+  hx_gemm_bulk_kernel<BC><<<grid, threads, smem, s>>>(fe, H, x, Yslot, B, mode, S, PW);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_hx_cell_gemm_bulk(const FeView &fe, const double *H, const double *x, double *Yslot, int B,
+                              int gather_mode, cudaStream_t s) {
+  if (B <= 2) hx_gemm_bulk_bc<2>(fe, H, x, Yslot, B, gather_mode, s);
+  else if (B <= 4) hx_gemm_bulk_bc<4>(fe, H, x, Yslot, B, gather_mode, s);
+  else if (B <= 8) hx_gemm_bulk_bc<8>(fe, H, x, Yslot, B, gather_mode, s);
+  else if (B <= 16) hx_gemm_bulk_bc<16>(fe, H, x, Yslot, B, gather_mode, s);
+  else if (B <= 32) hx_gemm_bulk_bc<32>(fe, H, x, Yslot, B, gather_mode, s);
+  else if (B <= 64) hx_gemm_bulk_bc<64>(fe, H, x, Yslot, B, gather_mode, s);
+  else throw StatusError(5, "block width above 64");
+}
+
+static void assemble_shape(int B, int &TR, int &cap) {
+  TR = std::max(8, std::min(128, 1024 / B));
+  cap = 2 * TR;   // ~1.6 slots per node on average
+}
+
+int assemble_blocks(const FeView &fe, int B) {
+  int TR, cap;
+  assemble_shape(B, TR, cap);
+  return (int)((fe.nnodes + TR - 1) / TR);
+}
+
+int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B, const AsmEpilogue &epi,
+                       int dot_blocks, cudaStream_t s) {
+  (void)dot_blocks;
+  if (B > NT) throw StatusError(5, "block width above 256");
+  static bool attr = false;
+  if (!attr) {
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_assemble_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     100 * 1024));
+    attr = true;
+  }
+  int TR, cap;
+  assemble_shape(B, TR, cap);
+  const int nb = assemble_blocks(fe, B);
+  if (fe.nhang > 0) {
+    hanging_sum_kernel<<<ceil_div((int64_t)fe.nhang * B, NT), NT, 0, s>>>(fe, Ycell, B);
+    INVDFT_LAUNCH_CHECK();
+  }
+  const size_t smem = sizeof(double) * (2 * (size_t)cap * B + 2 * (size_t)TR * B + TR) + sizeof(int) * 2 * (TR + 1);
+  hx_assemble_tile_kernel<<<nb, NT, smem, s>>>(fe, Ycell, out, B, epi, TR, cap);
+  INVDFT_LAUNCH_CHECK();
+  return nb;
 }
 
 void launch_scale_rows(const double *d, const double *x, double *y, int64_t n, int B, cudaStream_t s) {
@@ -868,7 +1401,8 @@ void launch_set_zero(const int *rows, int nrows, double *x, int B, cudaStream_t 
 }
 
 void launch_reduce_partials(const double *partial, int nparts, int width, double *out, cudaStream_t s) {
-  reduce_partials_kernel<<<ceil_div(width, NT), NT, 0, s>>>(partial, nparts, width, out);
+  if (width <= 0) return;
+  reduce_partials_kernel<<<width, NT, 0, s>>>(partial, nparts, width, out);
   INVDFT_LAUNCH_CHECK();
 }
 

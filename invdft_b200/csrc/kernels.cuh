@@ -7,6 +7,7 @@ namespace invdft {
 // Device-side view of the parent finite-element data.
 struct FeView {
   int n1, nd, nq;
+  int ldh;                  // leading dimension of a cell matrix column (nd rounded up to even)
   int64_t nc, nnodes;
   const double *phi;        // [n1][n1]: phi[q*n1+a] = l_a(gauss_q)
   const double *cell_h;     // [nc]
@@ -18,9 +19,19 @@ struct FeView {
   const double *cons_gw;    // weights * M^-1/2[master] (Lowdin gather)
   const int *cons_rows;     // [ncons]
   int ncons;
-  const int *sc_ptr;        // [nnodes+1] scatter CSR over nodes
-  const int *sc_src;        // entry -> cell*nd + local
-  const double *sc_w;       // condensation weight
+  // slot layout of cell results: row (cell, local) of a cell product is written
+  // to slot slot_of[cell*nd+local] (-1: Dirichlet row, dropped).  Free nodes own
+  // the contiguous slots [dptr[n], dptr[n+1]); rows of hanging nodes live in
+  // slots after those and reach their masters through (hslot, hw) lists.
+  const int *slot_of;       // [nc*nd]
+  const int *dptr;          // [nnodes+1]
+  const int *zptr;          // [nhang+1] slot ranges of the hanging nodes' rows
+  int nhang;
+  double *z;                // [nhang][B] scratch: summed rows of each hanging node
+  const int *hptr;          // [nnodes+1] (hanging node, weight) entries per master
+  const int *hslot;         // hanging-node index of each entry
+  const double *hw;
+  int *err;                 // device error word (bounded waits that gave up)
   const double *inv_sqrt_mass, *sqrt_mass;
 };
 
@@ -34,6 +45,12 @@ void launch_build_cell_h(const FeView &fe, const double *vks, const double *jxw,
                          double *H, cudaStream_t s);
 void launch_hx_cell_gemm(const FeView &fe, const double *H, const double *x, double *Ycell, int B,
                          int gather_mode, cudaStream_t s);
+// FP64 tensor-core (mma.sync m8n8k4 f64) variant
+void launch_hx_cell_dmma(const FeView &fe, const double *H, const double *x, double *Ycell, int B,
+                         int gather_mode, cudaStream_t s);
+// bulk-asynchronous staged variant (persistent CTAs, shared-memory panel ring)
+void launch_hx_cell_gemm_bulk(const FeView &fe, const double *H, const double *x, double *Yslot, int B,
+                              int gather_mode, cudaStream_t s);
 
 // Epilogue selector for the assembly kernel.
 struct AsmEpilogue {
@@ -48,8 +65,10 @@ struct AsmEpilogue {
   const double *minres_coef = nullptr;       // MINRES: beta/oldb per column (0 at itn 1)
   double *dot_partial = nullptr;             // MINRES: per-block column partials of v.y
 };
-void launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B,
-                        const AsmEpilogue &epi, int dot_blocks, cudaStream_t s);
+int assemble_blocks(const FeView &fe, int B);  // CTAs of launch_hx_assemble for width B
+// returns the number of CTAs (= MINRES dot partials written)
+int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B,
+                       const AsmEpilogue &epi, int dot_blocks, cudaStream_t s);
 
 void launch_scale_rows(const double *d, const double *x, double *y, int64_t n, int B, cudaStream_t s);
 void launch_distribute(const int *rows, const int *ptr, const int *masters, const double *w, int nrows,

@@ -222,6 +222,20 @@ invdft_status invdft_bfgs_solve(invdft_ctx *ctx, double *pot, int32_t max_iter, 
                                 int32_t line_search_iters, double line_search_tol,
                                 int32_t history, double *losses, int32_t *n_evals);
 
+/* Per-column dot products out[j] = sum_i a[i*B+j] b[i*B+j] of device blocks
+ * [n][B], computed on `stream` (a cudaStream_t, NULL = default stream) without
+ * allocating anything.  No counterpart in the reference: it serves callers that
+ * must not let a library allocate device memory while they run (an outer
+ * L-BFGS or Krylov driver whose vectors live in its own device pool).  Needs no
+ * context.  Scratch is a static device array of 296 x 64 doubles held by every
+ * GPU that loads the library, so B must be in [1, 64] (BAD_ARG otherwise, with
+ * the reason in invdft_last_error(NULL)).  The first call on a device looks up
+ * the array's device address and should come before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race.  Asynchronous
+ * with respect to the host; d_out [B] is device memory. */
+invdft_status invdft_coldot_noalloc(const double *d_a, const double *d_b, int64_t n, int32_t B,
+                                    double *d_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

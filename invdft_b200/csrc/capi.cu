@@ -40,6 +40,7 @@ template <class F> invdft_status guard(invdft_ctx *ctx, F &&f) {
 
 namespace invdft {
 int64_t child_node_count(invdft_ctx *ctx) { return (ctx && ctx->c) ? ctx->c->ncn : -1; }
+void set_thread_error(const std::string &msg) { g_create_error = msg; }
 // Implemented in bfgs.cpp
 invdft_status bfgs_solve(invdft_ctx *ctx, double *pot, int max_iter, double tol, int ls_iters, double ls_tol,
                          int history, double *losses, int *n_evals);

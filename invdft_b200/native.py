@@ -23,7 +23,7 @@ EXPORTED = [
     "invdft_set_potential", "invdft_hx", "invdft_adjoint_update_psi", "invdft_adjoint_compute_rhs",
     "invdft_adjoint_vmult", "invdft_adjoint_precondition_jacobi",
     "invdft_adjoint_precondition_jacobi_sqrt", "invdft_adjoint_distribute_x", "invdft_adjoint_solve",
-    "invdft_bfgs_solve",
+    "invdft_bfgs_solve", "invdft_coldot_noalloc",
 ]
 
 
@@ -123,6 +123,7 @@ def load() -> C.CDLL:
         "invdft_adjoint_solve": (C.c_int, [vp, vp, C.c_double, C.c_int32, _P(C.c_int32)]),
         "invdft_bfgs_solve": (C.c_int, [vp, _f64p, C.c_int32, C.c_double, C.c_int32, C.c_double,
                                         C.c_int32, _f64p, _P(C.c_int32)]),
+        "invdft_coldot_noalloc": (C.c_int, [vp, vp, C.c_int64, C.c_int32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

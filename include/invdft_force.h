@@ -136,6 +136,8 @@ typedef struct {
   int64_t n_launches;        /* kernels this evaluation launched */
   int32_t degree;            /* Chebyshev filter degree used */
   double upper_bound;        /* Lanczos upper bound of the spectrum */
+  double device_bytes;       /* device memory held by the library after the evaluation */
+  double device_bytes_peak;  /* its high-water mark */
 } invdft_force_stats;
 
 /* Defaults of the reference's parameters. */
@@ -176,8 +178,16 @@ invdft_status invdft_get_psi(invdft_ctx *ctx, double *psi);           /* nodal [
 invdft_status invdft_get_density(invdft_ctx *ctx, double *rho);       /* [n_cells*n1^3] total */
 invdft_status invdft_get_child_quad_products(invdft_ctx *ctx, double *S); /* [n_child_cells*8] */
 
-/* Forward map only: solveEigen (:1315-1477) + computeRhoFromPSI (:748-758). */
+/* Forward half of getForceVector: distribute v_xc, solveEigen (:1315-1477),
+ * computeRhoFromPSI (:748-758), drho and the loss (:776-912); stats->loss
+ * receives L.  The eigenvectors stay in the context (stored once) for
+ * invdft_force_backward.  pot's constrained entries are zeroed on exit. */
 invdft_status invdft_solve_eigen(invdft_ctx *ctx, double *pot, invdft_force_stats *stats);
+/* Backward half of getForceVector for the last invdft_solve_eigen: the block
+ * adjoint solves and the projection (:914-1246) giving force = dL/dv_xc
+ * [n_child_nodes].  invdft_solve_eigen + invdft_force_backward ==
+ * invdft_force_eval. */
+invdft_status invdft_force_backward(invdft_ctx *ctx, double *force, invdft_force_stats *stats);
 
 /* --- building blocks, exposed for the adjoint interface and for tests --- */
 

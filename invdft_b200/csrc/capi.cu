@@ -166,16 +166,19 @@ invdft_status invdft_get_child_quad_products(invdft_ctx *ctx, double *S) {
 invdft_status invdft_solve_eigen(invdft_ctx *ctx, double *pot, invdft_force_stats *stats) {
   return guard(ctx, [&](invdft::Context &c) {
     if (!pot) throw invdft::StatusError(INVDFT_BAD_ARG, "null potential");
-    c.pot_d.upload(pot, c.ncn, c.stream);
-    c.solve_eigen(c.pot_d.p, stats);
-    double sums[4];
-    c.density_and_loss(sums);
-    if (stats) {
-      stats->loss = sums[0];
-      stats->loss_unweighted = sums[1];
-      stats->l1_error = sums[2];
-      stats->int_rho_veff = sums[3];
-    }
+    invdft_force_stats local{};
+    invdft_force_stats *st = stats ? stats : &local;
+    std::memset(st, 0, sizeof(*st));
+    c.forward(pot, st);
+  });
+}
+
+invdft_status invdft_force_backward(invdft_ctx *ctx, double *force, invdft_force_stats *stats) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!force) throw invdft::StatusError(INVDFT_BAD_ARG, "null force");
+    invdft_force_stats local{};
+    invdft_force_stats *st = stats ? stats : &local;
+    c.backward(force, st);
   });
 }
 

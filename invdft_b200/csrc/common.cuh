@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -28,6 +29,16 @@ struct StatusError : std::runtime_error {
 
 #define INVDFT_LAUNCH_CHECK() INVDFT_CUDA(cudaGetLastError())
 
+// Bytes currently held by all DevBuf allocations of this process.
+inline std::atomic<long long> &device_bytes() {
+  static std::atomic<long long> b{0};
+  return b;
+}
+inline std::atomic<long long> &device_bytes_peak() {
+  static std::atomic<long long> b{0};
+  return b;
+}
+
 // Owning device buffer.
 template <typename T> struct DevBuf {
   T *p = nullptr;
@@ -52,11 +63,18 @@ template <typename T> struct DevBuf {
         (void)cudaGetLastError();
         throw StatusError(4, "cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes failed");
       }
+      const long long now = device_bytes() += (long long)(count * sizeof(T));
+      long long pk = device_bytes_peak().load();
+      while (now > pk && !device_bytes_peak().compare_exchange_weak(pk, now)) {
+      }
     }
   }
   void ensure(size_t count) { if (count > n) alloc(count); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      cudaFree(p);
+      device_bytes() -= (long long)(n * sizeof(T));
+    }
     p = nullptr; n = 0;
   }
   void upload(const T *h, size_t count, cudaStream_t s = 0) {

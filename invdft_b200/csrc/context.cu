@@ -982,13 +982,13 @@ struct StageTimer {
 };
 }  // namespace
 
-void Context::eval(double *pot, double *force, double *loss, invdft_force_stats *st) {
-  invdft_force_stats local{};
-  if (!st) st = &local;
-  std::memset(st, 0, sizeof(*st));
+// Forward half of getForceVector: distribute v_xc, solveEigen, rho, drho, loss
+// (InverseDFTSolverFunction.cpp:671-912).  The eigenvectors stay in the context
+// (stored once) for the backward half.
+void Context::forward(double *pot, invdft_force_stats *st) {
   n_hx = 0;
   n_hx_cols = 0;
-  const long long launches0 = launch_count();
+  fwd_launches0 = launch_count();
   profile_begin();
   for (int64_t i = 0; i < ncn; ++i)
     if (!std::isfinite(pot[i])) throw StatusError(INVDFT_NONFINITE, "non-finite entry in the potential");
@@ -1005,6 +1005,22 @@ void Context::eval(double *pot, double *force, double *loss, invdft_force_stats 
   st->l1_error = sums[2];
   st->int_rho_veff = sums[3];
   if (!std::isfinite(sums[0])) throw StatusError(INVDFT_NONFINITE, "non-finite loss");
+  last_loss = sums[0];
+  have_forward = true;
+  // zero the constrained entries of the potential on exit (:1295-1298)
+  for (int64_t r : cchild.h_rows) pot[r] = 0.0;
+  loss_prev = sums[0];
+  ++counter;
+  st->n_hx_calls = n_hx;
+  st->n_hx_columns = n_hx_cols;
+}
+
+// Backward half: per block updateInputPsi, block MINRES, distributeX, adjoint
+// constraints, psi.p at the child quadrature points, projection onto the v_xc
+// nodes (InverseDFTSolverFunction.cpp:914-1246).  Uses the eigenvectors and u
+// of the last forward half; keeps no Krylov vectors afterwards.
+void Context::backward(double *force, invdft_force_stats *st) {
+  if (!have_forward) throw StatusError(INVDFT_NOT_READY, "backward needs a forward evaluation first");
   S.zero(stream);
   StageTimer t_adj(stream);
   double t_transfer = 0.0;
@@ -1045,23 +1061,28 @@ void Context::eval(double *pot, double *force, double *loss, invdft_force_stats 
   t_transfer += t_f.stop();
   st->ms_adjoint = t_adj.stop() - t_transfer;
   st->ms_transfer = t_transfer;
-  // zero constrained entries of force (hanging, :1246) and pot (:1295-1298)
-  for (int64_t r : cchild.h_rows) {
-    force[r] = 0.0;
-    pot[r] = 0.0;
-  }
-  *loss = sums[0];
+  for (int64_t r : cchild.h_rows) force[r] = 0.0;   // (:1246)
   st->adjoint_tol = adjoint_tol;
   st->minres_iters_max = itmax;
   st->minres_iters_sum = itsum;
   st->n_blocks = nblk;
   st->n_hx_calls = n_hx;
   st->n_hx_columns = n_hx_cols;
-  loss_prev = sums[0];
-  ++counter;
-  st->n_launches = launch_count() - launches0;
+  st->loss = last_loss;
+  st->n_launches = launch_count() - fwd_launches0;
+  st->device_bytes = (double)device_bytes().load();
+  st->device_bytes_peak = (double)device_bytes_peak().load();
   profile_end(st);
   check_device_error();
+}
+
+void Context::eval(double *pot, double *force, double *loss, invdft_force_stats *st) {
+  invdft_force_stats local{};
+  if (!st) st = &local;
+  std::memset(st, 0, sizeof(*st));
+  forward(pot, st);
+  backward(force, st);
+  *loss = last_loss;
 }
 
 }  // namespace invdft

@@ -116,8 +116,13 @@ class Context {
   void adj_precondition(double *d_dst, const double *d_src, bool sqrt_version);
   void adj_distribute_x(double *d_x);
   void adj_minres(double *d_x, double tol, int maxit, std::vector<int> &iters);
-  // full evaluation
+  // full evaluation = forward half + backward half
+  void forward(double *pot, invdft_force_stats *st);
+  void backward(double *force, invdft_force_stats *st);
   void eval(double *pot, double *force, double *loss, invdft_force_stats *st);
+  bool have_forward = false;
+  double last_loss = 0.0;
+  long long fwd_launches0 = 0;
   void accumulate_child_products(const double *d_psi, const double *d_p, int Bw);
 
  private:

@@ -561,7 +561,7 @@ __global__ void __launch_bounds__(NT) hx_assemble_tile_kernel(FeView fe, const d
   // weighted rows of the hanging nodes feeding this tile's masters, all
   // loaded in one wave (z is small and L2-resident)
   const int h0 = hp[0], h1 = hp[rows];
-  const bool hstaged = (h1 - h0) <= cap_slots;
+  const bool hstaged = (h1 - h0) <= cap_slots;   // hv holds cap_slots rows of B
   if (hstaged) {
     constexpr int U = 8;
     const int n = (h1 - h0) * B;
@@ -589,14 +589,35 @@ __global__ void __launch_bounds__(NT) hx_assemble_tile_kernel(FeView fe, const d
       const int64_t n = r0 + lr;
       const int d0 = dp[lr], d1 = dp[lr + 1];
       double acc = 0.0;
-      if (staged)
+      if (staged) {
         for (int sl = d0; sl < d1; ++sl) acc += seg[(sl - s0) * B + j];
-      else
-        for (int sl = d0; sl < d1; ++sl) acc += Ycell[(int64_t)sl * B + j];
-      if (hstaged)
+      } else {
+        for (int sl = d0; sl < d1; sl += 8) {      // eight independent loads in flight
+          double v[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) v[u] = (sl + u < d1) ? Ycell[(int64_t)(sl + u) * B + j] : 0.0;
+#pragma unroll
+          for (int u = 0; u < 8; ++u) acc += v[u];
+        }
+      }
+      if (hstaged) {
         for (int k = hp[lr]; k < hp[lr + 1]; ++k) acc += hv[(k - h0) * B + j];
-      else
-        for (int k = hp[lr]; k < hp[lr + 1]; ++k) acc = fma(fe.hw[k], fe.z[(int64_t)fe.hslot[k] * B + j], acc);
+      } else {
+        const int k1 = hp[lr + 1];
+        for (int k = hp[lr]; k < k1; k += 8) {
+          int hs[8];
+          double w[8], v[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            hs[u] = (k + u < k1) ? fe.hslot[k + u] : 0;
+            w[u] = (k + u < k1) ? fe.hw[k + u] : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) v[u] = fe.z[(int64_t)hs[u] * B + j];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) acc += w[u] * v[u];
+        }
+      }
       acc *= ism[lr];
       const int64_t idx = n * B + j;
       const int li = lr * B + j;

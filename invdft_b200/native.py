@@ -20,6 +20,7 @@ EXPORTED = [
     "invdft_default_params", "invdft_force_create", "invdft_force_destroy", "invdft_last_error",
     "invdft_set_params", "invdft_set_profiling", "invdft_set_subspace", "invdft_force_eval", "invdft_dot", "invdft_get_eigen",
     "invdft_get_psi", "invdft_get_density", "invdft_get_child_quad_products", "invdft_solve_eigen",
+    "invdft_force_backward",
     "invdft_set_potential", "invdft_hx", "invdft_adjoint_update_psi", "invdft_adjoint_compute_rhs",
     "invdft_adjoint_vmult", "invdft_adjoint_precondition_jacobi",
     "invdft_adjoint_precondition_jacobi_sqrt", "invdft_adjoint_distribute_x", "invdft_adjoint_solve",
@@ -77,7 +78,7 @@ class Stats(C.Structure):
         ("ms_density", C.c_double), ("ms_adjoint", C.c_double), ("ms_transfer", C.c_double),
         ("n_cell_gemm", C.c_int32), ("ms_cell_gemm", C.c_double), ("cell_gemm_bytes", C.c_double),
         ("cell_gemm_flops", C.c_double), ("n_launches", C.c_int64), ("degree", C.c_int32),
-        ("upper_bound", C.c_double),
+        ("upper_bound", C.c_double), ("device_bytes", C.c_double), ("device_bytes_peak", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -111,6 +112,7 @@ def load() -> C.CDLL:
         "invdft_get_density": (C.c_int, [vp, _f64p]),
         "invdft_get_child_quad_products": (C.c_int, [vp, _f64p]),
         "invdft_solve_eigen": (C.c_int, [vp, _f64p, _P(Stats)]),
+        "invdft_force_backward": (C.c_int, [vp, _f64p, _P(Stats)]),
         "invdft_set_potential": (C.c_int, [vp, _f64p]),
         "invdft_hx": (C.c_int, [vp, vp, vp, C.c_int32]),
         "invdft_adjoint_update_psi": (C.c_int, [vp, vp, _f64p, vp, _P(C.c_int32), _P(C.c_int32),

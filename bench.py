@@ -176,6 +176,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c1_c2h4")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-fp64-compare", action="store_true",
+                    help="do not time the FP64 path on the same trajectory")
     ap.add_argument("--cpu-sample-cells", type=int, default=400)
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample (profiling runs)")
     args = ap.parse_args()
@@ -259,6 +261,24 @@ def main():
     achieved = gemm_bytes / (gemm_ms / 1000.0) / 1e9 if gemm_ms > 0 else None
     per_launch_traffic = _traffic_from_profiles(f"{args.config}:{args.precision}")
     launches = int(sum(s["n_launches"] for s in stats))
+    fp64_cmp = None
+    if args.precision == "mixed" and not args.no_fp64_compare:
+        fn64 = InverseDFTSolverFunction(P, force_params("fp64"))
+        for k in range(args.warmup):
+            fn64.get_force_vector(trajectory(P, k, total).copy())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        f64_stats = []
+        for k in range(args.warmup, total):
+            f64_stats.append(fn64.get_force_vector(trajectory(P, k, total).copy())[2])
+        e1.record()
+        torch.cuda.synchronize()
+        v64, _, ms64 = aggregate(e0.elapsed_time(e1), 1.0, args.steps, world, dist)
+        fp64_cmp = {"value": v64, "ms_per_step": ms64 / args.steps, "passes": [s["passes"] for s in f64_stats],
+                    "speedup_mixed_vs_fp64": value / v64,
+                    "max_abs_loss_diff_vs_fp64": max(abs(a["loss"] - b["loss"]) for a, b in zip(stats, f64_stats))}
+        fn64.close()
     if rank == 0:
         if args.no_cpu_baseline:
             cpu_v, cpu_meta = None, dict(kind="port", cores=threads, sample="skipped (--no-cpu-baseline)")
@@ -268,7 +288,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "force-evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 (FP32-stored cell matrices in the filter)",
             "data": "synthetic (seeded; see invdft_b200/problem/system.py)",
             "config": {
                 "workload": f"{args.config}: C2H4-like, FE order {P.p}, {P.n_nodes} DoF, {P.n_cells} cells, "
@@ -278,6 +298,8 @@ def main():
                 f"{P.n_cells * P.nd * P.nd * 8 / 1e9:.2f} GB)",
                 "step": "one getForceVector at a new v_xc on the path guess -> v_xc*",
                 "chebyshev_passes": [s["passes"] for s in stats],
+                "chebyshev_passes_fp32_stored": [s["passes_low"] for s in stats],
+                "fp64_same_trajectory": fp64_cmp,
                 "chebyshev_degree": [s["degree"] for s in stats],
                 "spectrum_upper_bound": stats[-1]["upper_bound"],
                 "minres_iters_max": [s["minres_iters_max"] for s in stats],

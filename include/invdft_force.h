@@ -4,8 +4,10 @@
  * The library replaces, for one GPU, the reference's
  *   InverseDFTSolverFunction<p,pe,mem>          (include/InverseDFTSolverFunction.h:51-384)
  *   MultiVectorAdjointLinearSolverProblem<mem>  (include/MultiVectorAdjointLinearSolverProblem.h:15-214)
- * behind plain pointers and sizes.  All arithmetic on the path is FP64 unless
- * the context is switched to INVDFT_PRECISION_MIXED.
+ * behind plain pointers and sizes.  All arithmetic on the path is FP64.  With
+ * INVDFT_PRECISION_MIXED the Chebyshev filter streams the cell matrices stored
+ * in FP32 (products still accumulated in FP64 on the tensor cores) until the
+ * residual reaches mixed_residual_floor; everything else stays FP64.
  *
  * Vectors ("multi-vectors") are row-major [n_nodes][B]: node index slowest,
  * vector index fastest, as the reference's dftfe::linearAlgebra::MultiVector
@@ -109,6 +111,8 @@ typedef struct {
   double factor_lda;              /* FACTOR FOR LDA VXC */
   int32_t lanczos_steps;          /* steps of the spectrum-bound Lanczos run */
   int32_t precision;              /* invdft_precision */
+  double mixed_residual_floor;    /* MIXED: filter with FP32-stored cell matrices until the max
+                                     residual falls below this or stalls, then in FP64 */
 } invdft_params;
 
 typedef struct {
@@ -138,6 +142,7 @@ typedef struct {
   double upper_bound;        /* Lanczos upper bound of the spectrum */
   double device_bytes;       /* device memory held by the library after the evaluation */
   double device_bytes_peak;  /* its high-water mark */
+  int32_t passes_low;        /* Chebyshev passes filtered with FP32-stored cell matrices */
 } invdft_force_stats;
 
 /* Defaults of the reference's parameters. */

@@ -67,6 +67,7 @@ void invdft_default_params(invdft_params *p) {
   p->factor_lda = 0.0;
   p->lanczos_steps = 20;
   p->precision = INVDFT_PRECISION_FP64;
+  p->mixed_residual_floor = 1e-4;
 }
 
 invdft_status invdft_force_create(const invdft_problem_desc *desc, const invdft_params *params,

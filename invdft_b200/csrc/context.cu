@@ -402,6 +402,7 @@ void Context::set_params(const invdft_params *pp) {
   check(pp->block_size >= 0, "block_size must be >= 0");
   check(pp->lanczos_steps >= 2, "lanczos_steps must be >= 2");
   check(pp->precision == INVDFT_PRECISION_FP64 || pp->precision == INVDFT_PRECISION_MIXED, "bad precision");
+  check(pp->mixed_residual_floor >= 0.0, "mixed_residual_floor must be >= 0");
   prm = *pp;
 }
 
@@ -449,17 +450,18 @@ void Context::set_subspace(const double *Xh) {
 // ---------------------------------------------------------------------------
 // Hamiltonian application and the eigensolver
 // ---------------------------------------------------------------------------
-void Context::cell_gemm(const double *d_x, int Bw) {
+void Context::cell_gemm(const double *d_x, int Bw, bool low) {
   const bool rec = profile && ev_used + 2 <= (int)ev_pool.size();
   if (rec) INVDFT_CUDA(cudaEventRecord(ev_pool[ev_used], stream));
-  if (hx_variant == 0) launch_hx_cell_dmma(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
+  if (low) launch_hx_cell_dmma_f32(fe, H32.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
+  else if (hx_variant == 0) launch_hx_cell_dmma(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
   else if (hx_variant == 2) launch_hx_cell_gemm_bulk(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
   else launch_hx_cell_gemm(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
   if (rec) {
     INVDFT_CUDA(cudaEventRecord(ev_pool[ev_used + 1], stream));
     ev_used += 2;
     // algorithmic traffic: cell matrices once, the block once, the cell results once
-    prof_bytes += 8.0 * ((double)nc * nd * nd + (double)nn * Bw + (double)nc * nd * Bw);
+    prof_bytes += (low ? 4.0 : 8.0) * (double)nc * nd * nd + 8.0 * ((double)nn * Bw + (double)nc * nd * Bw);
     prof_flops += 2.0 * (double)nc * nd * nd * Bw;
   }
 }
@@ -503,6 +505,12 @@ void Context::set_potential_device(double *d_pot) {
   launch_child_to_parent_quad(cv, d_pot, v_base.p, v_lda.p, prm.factor_lda, vks.p, nc * nq, stream);
   launch_build_cell_h(fe, vks.p, jxw.p, Kref.p, H.p, stream);
   have_H = true;
+  have_H32 = false;
+  if (prm.precision == INVDFT_PRECISION_MIXED) {
+    H32.ensure(H.n);
+    launch_narrow(H.p, H32.p, (int64_t)H.n, stream);
+    have_H32 = true;
+  }
 }
 
 namespace {
@@ -583,7 +591,7 @@ int auto_degree(double upper_bound) {
   return (int)std::min(500.0, std::max(24.0, m));
 }
 
-void Context::chfsi_pass(double a, double b, double a0, std::vector<double> &res) {
+void Context::chfsi_pass(double a, double b, double a0, std::vector<double> &res, bool low) {
   const int m = prm.cheb_degree > 0 ? prm.cheb_degree : auto_degree(b);
   const double e = (b - a) / 2.0, c = (b + a) / 2.0;
   double sigma = e / (a0 - c);
@@ -591,7 +599,7 @@ void Context::chfsi_pass(double a, double b, double a0, std::vector<double> &res
   // Chebyshev recurrence on three rotating buffers: P0 = X, P1 = first step
   double *P0 = X.p, *P1 = Yb.p, *P2 = Zb.p;
   {
-    cell_gemm(P0, N);
+    cell_gemm(P0, N, low);
     AsmEpilogue epi;
     epi.kind = AsmEpilogue::CHEB;
     epi.alpha = sigma1 / e;
@@ -604,7 +612,7 @@ void Context::chfsi_pass(double a, double b, double a0, std::vector<double> &res
   }
   for (int k = 2; k <= m; ++k) {
     const double sigma2 = 1.0 / (gamma - sigma);
-    cell_gemm(P1, N);
+    cell_gemm(P1, N, low);
     AsmEpilogue epi;
     epi.kind = AsmEpilogue::CHEB;
     epi.alpha = 2.0 * sigma2 / e;
@@ -675,9 +683,13 @@ void Context::solve_eigen(double *d_pot, invdft_force_stats *st) {
   set_potential_device(d_pot);
   double lo, b;
   lanczos_bounds(lo, b);
-  int passes = 0;
-  double maxres = 0.0;
+  int passes = 0, passes_low = 0;
+  double maxres = 0.0, prev_maxres = 1e300;
   std::vector<double> res;
+  // precision ladder: filter with the FP32-stored cell matrices while the
+  // residual keeps falling and stays above the floor, then finish in FP64
+  // (Rayleigh-Ritz and the residual norms are always FP64)
+  bool low = prm.precision == INVDFT_PRECISION_MIXED && have_H32;
   for (;;) {
     double a, a0;
     if (!have_eig) {
@@ -687,7 +699,7 @@ void Context::solve_eigen(double *d_pot, invdft_force_stats *st) {
       a0 = eig.front();
       a = eig.back();
     }
-    chfsi_pass(a, b, a0, res);
+    chfsi_pass(a, b, a0, res, low);
     mu = fermi_energy(eig, n_electrons, kT);
     occ.resize(N);
     int homo = 0;
@@ -699,12 +711,16 @@ void Context::solve_eigen(double *d_pot, invdft_force_stats *st) {
     for (int i = 0; i < N; ++i)
       if (occ[i] > prm.frac_occ_tol || i <= homo + prm.additional_states) maxres = std::max(maxres, res[i]);
     ++passes;
+    if (low) ++passes_low;
     if (!(maxres > tol_cheb && passes < prm.max_cheb_passes)) break;
+    if (low && (maxres < prm.mixed_residual_floor || maxres > 0.5 * prev_maxres)) low = false;
+    prev_maxres = maxres;
   }
   // nodal eigenvectors psi = C M^-1/2 X
   launch_scale_rows(invsqrtM.p, X.p, psi.p, nn, N, stream);
   launch_distribute(cpsi.rows.p, cpsi.ptr.p, cpsi.masters.p, cpsi.w.p, cpsi.n, psi.p, N, stream);
   if (st) {
+    st->passes_low = passes_low;
     st->degree = prm.cheb_degree > 0 ? prm.cheb_degree : auto_degree(b);
     st->upper_bound = b;
     st->passes = passes;
@@ -867,14 +883,35 @@ void Context::adj_distribute_x(double *d_x) {
   }
 }
 
+namespace {
+__global__ void gather_columns_kernel(const double *__restrict__ src, int bsrc, const int *__restrict__ idx,
+                                      double *__restrict__ dst, int bdst, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n * bdst) return;
+  const int64_t r = i / bdst;
+  dst[i] = src[r * bsrc + idx[i % bdst]];
+}
+__global__ void scatter_columns_kernel(const double *__restrict__ src, int bsrc, const int *__restrict__ idx,
+                                       double *__restrict__ dst, int bdst, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n * bsrc) return;
+  const int64_t r = i / bsrc;
+  dst[r * bdst + idx[i % bsrc]] = src[i];
+}
+}  // namespace
+
+// Block MINRES with per-column convergence.  The state lives in a compact
+// block of the columns that are still active (column map cmap -> original
+// column); when enough columns have converged the block is re-packed, so
+// converged and zero right-hand-side columns cost nothing.  Columns never
+// interact, so the arithmetic of an active column is the same as in the
+// uncompacted solve.
 void Context::adj_minres(double *d_x, double tol, int maxit, std::vector<int> &iters) {
   if (!psi_ready) throw StatusError(INVDFT_NOT_READY, "updateInputPsi has not been called");
   const int Bw = B;
   const size_t v = (size_t)nn * Bw;
   adj_compute_rhs(m_b.p);
   INVDFT_CUDA(cudaMemsetAsync(d_x, 0, v * sizeof(double), stream));
-  INVDFT_CUDA(cudaMemsetAsync(m_w.p, 0, v * sizeof(double), stream));
-  INVDFT_CUDA(cudaMemsetAsync(m_w2.p, 0, v * sizeof(double), stream));
   MinresState st;
   double *sc = m_scal.p;
   st.beta = sc + 0 * 64; st.oldb = sc + 1 * 64; st.dbar = sc + 2 * 64; st.epsln = sc + 3 * 64;
@@ -890,36 +927,99 @@ void Context::adj_minres(double *d_x, double tol, int maxit, std::vector<int> &i
   launch_minres_init(m_b.p, diagA.p, m_r1.p, m_r2.p, m_y.p, nn, Bw, partial.p, nblocks_red, stream);
   launch_reduce_partials(partial.p, nblocks_red, Bw, st.beta2, stream);
   launch_minres_init_scalars(st, st.beta2, Bw, stream);
-  std::vector<int> act(Bw);
+  std::vector<int> iters_full(Bw, 0);
+  std::vector<int> cmap(Bw);
+  for (int j = 0; j < Bw; ++j) cmap[j] = j;
+  int Bc = Bw;
+  std::vector<double> h_eps(h_eig);
+  DevBuf<double> eps_c;
+  eps_c.upload(h_eps, stream);
+  DevBuf<int> d_idx;
+  auto scatter_x = [&]() {
+    d_idx.upload(cmap, stream);
+    scatter_columns_kernel<<<ceil_div((int64_t)nn * Bc, 256), 256, 0, stream>>>(m_xc.p, Bc, d_idx.p, d_x, Bw, nn);
+    INVDFT_LAUNCH_CHECK();
+    count_launch();
+  };
+  // re-pack the state onto the columns `keep` (positions in the current block)
+  auto compact = [&](const std::vector<int> &keep) {
+    const int Bn = (int)keep.size();
+    scatter_x();
+    std::vector<int> it_now(Bc);
+    INVDFT_CUDA(cudaMemcpyAsync(it_now.data(), st.iters, sizeof(int) * Bc, cudaMemcpyDeviceToHost, stream));
+    std::vector<double> hs(16 * 64);
+    std::vector<int> hf(3 * 64);
+    INVDFT_CUDA(cudaMemcpyAsync(hs.data(), m_scal.p, sizeof(double) * 16 * 64, cudaMemcpyDeviceToHost, stream));
+    INVDFT_CUDA(cudaMemcpyAsync(hf.data(), m_flags.p, sizeof(int) * 3 * 64, cudaMemcpyDeviceToHost, stream));
+    INVDFT_CUDA(cudaStreamSynchronize(stream));
+    for (int k = 0; k < Bc; ++k) iters_full[cmap[k]] = it_now[k];
+    d_idx.upload(keep, stream);
+    DevBuf<double> *vecs[] = {&m_r1, &m_r2, &m_y, &m_w, &m_w2, &m_xc};
+    for (DevBuf<double> *V : vecs) {
+      gather_columns_kernel<<<ceil_div((int64_t)nn * Bn, 256), 256, 0, stream>>>(V->p, Bc, d_idx.p, m_tmp.p, Bn, nn);
+      INVDFT_LAUNCH_CHECK();
+      count_launch();
+      std::swap(V->p, m_tmp.p);
+      std::swap(V->n, m_tmp.n);
+    }
+    std::vector<double> hs2(16 * 64, 0.0);
+    std::vector<int> hf2(3 * 64, 0);
+    std::vector<int> cmap2(Bn);
+    std::vector<double> eps2(Bn);
+    for (int k = 0; k < Bn; ++k) {
+      for (int a = 0; a < 16; ++a) hs2[a * 64 + k] = hs[a * 64 + keep[k]];
+      for (int a = 0; a < 3; ++a) hf2[a * 64 + k] = hf[a * 64 + keep[k]];
+      cmap2[k] = cmap[keep[k]];
+      eps2[k] = h_eps[keep[k]];
+    }
+    INVDFT_CUDA(cudaMemcpyAsync(m_scal.p, hs2.data(), sizeof(double) * 16 * 64, cudaMemcpyHostToDevice, stream));
+    INVDFT_CUDA(cudaMemcpyAsync(m_flags.p, hf2.data(), sizeof(int) * 3 * 64, cudaMemcpyHostToDevice, stream));
+    cmap = cmap2;
+    h_eps = eps2;
+    eps_c.upload(h_eps, stream);
+    Bc = Bn;
+    INVDFT_CUDA(cudaStreamSynchronize(stream));
+  };
+  m_xc.ensure(v);
+  m_tmp.ensure(v);
+  INVDFT_CUDA(cudaMemsetAsync(m_xc.p, 0, v * sizeof(double), stream));
+  INVDFT_CUDA(cudaMemsetAsync(m_w.p, 0, v * sizeof(double), stream));
+  INVDFT_CUDA(cudaMemsetAsync(m_w2.p, 0, v * sizeof(double), stream));
+  std::vector<int> act(64);
   const int check_every = 8;
   for (int itn = 1; itn <= maxit; ++itn) {
     if ((itn - 1) % check_every == 0) {
-      INVDFT_CUDA(cudaMemcpyAsync(act.data(), st.active, sizeof(int) * Bw, cudaMemcpyDeviceToHost, stream));
+      INVDFT_CUDA(cudaMemcpyAsync(act.data(), st.active, sizeof(int) * Bc, cudaMemcpyDeviceToHost, stream));
       INVDFT_CUDA(cudaStreamSynchronize(stream));
-      bool any = false;
-      for (int b = 0; b < Bw; ++b) any |= act[b] != 0;
-      if (!any) break;
+      std::vector<int> keep;
+      for (int k = 0; k < Bc; ++k)
+        if (act[k]) keep.push_back(k);
+      if (keep.empty()) break;
+      if ((int)keep.size() < Bc && (4 * (int)keep.size() <= 3 * Bc || (int)keep.size() + 2 <= Bc)) compact(keep);
     }
-    launch_minres_v(m_y.p, st, m_v.p, nn, Bw, stream);
-    cell_gemm(m_v.p, Bw);
+    launch_minres_v(m_y.p, st, m_v.p, nn, Bc, stream);
+    cell_gemm(m_v.p, Bc);
     AsmEpilogue epi;
     epi.kind = AsmEpilogue::MINRES;
     epi.in = m_v.p;
     epi.prev = m_r1.p;
-    epi.eps = a_eig.p;
+    epi.eps = eps_c.p;
     epi.minres_coef = st.coef1;
     epi.dot_partial = partial.p;
-    const int nparts = launch_hx_assemble(fe, Ycell.p, m_yn.p, Bw, epi, nblocks_red, stream);
-    launch_reduce_partials(partial.p, nparts, Bw, st.alfa, stream);
+    const int nparts = launch_hx_assemble(fe, Ycell.p, m_yn.p, Bc, epi, nblocks_red, stream);
+    launch_reduce_partials(partial.p, nparts, Bc, st.alfa, stream);
     n_hx++;
-    n_hx_cols += Bw;
-    launch_minres_update1(m_r1.p, m_r2.p, m_y.p, m_yn.p, diagA.p, st, nn, Bw, partial.p, nblocks_red, stream);
-    launch_minres_scalars(st, Bw, itn, stream);
-    launch_minres_update2(d_x, m_w.p, m_w2.p, m_v.p, st, nn, Bw, stream);
+    n_hx_cols += Bc;
+    launch_minres_update1(m_r1.p, m_r2.p, m_y.p, m_yn.p, diagA.p, st, nn, Bc, partial.p, nblocks_red, stream);
+    launch_minres_scalars(st, Bc, itn, stream);
+    launch_minres_update2(m_xc.p, m_w.p, m_w2.p, m_v.p, st, nn, Bc, stream);
   }
-  iters.assign(Bw, 0);
-  INVDFT_CUDA(cudaMemcpyAsync(iters.data(), st.iters, sizeof(int) * Bw, cudaMemcpyDeviceToHost, stream));
+  scatter_x();
+  std::vector<int> it_now(Bc);
+  INVDFT_CUDA(cudaMemcpyAsync(it_now.data(), st.iters, sizeof(int) * Bc, cudaMemcpyDeviceToHost, stream));
   INVDFT_CUDA(cudaStreamSynchronize(stream));
+  for (int k = 0; k < Bc; ++k) iters_full[cmap[k]] = it_now[k];
+  iters = iters_full;
   last_iters = iters;
   adj_distribute_x(d_x);
 }

@@ -80,7 +80,9 @@ class Context {
   std::vector<cudaEvent_t> ev_pool;
   int ev_used = 0;
   double prof_bytes = 0.0, prof_flops = 0.0;
-  void cell_gemm(const double *d_x, int Bw);
+  void cell_gemm(const double *d_x, int Bw, bool low = false);
+  DevBuf<float> H32;               // FP32 copy of the cell matrices (mixed precision)
+  bool have_H32 = false;
   void profile_begin();
   void profile_end(invdft_force_stats *st);
 
@@ -93,7 +95,7 @@ class Context {
   std::vector<int> pairs, pair_ptr, pair_j;
   DevBuf<int> d_pairs, d_pair_ptr, d_pair_j;
   // MINRES buffers
-  DevBuf<double> m_r1, m_r2, m_y, m_v, m_w, m_w2, m_yn, m_b, m_x, m_p;
+  DevBuf<double> m_r1, m_r2, m_y, m_v, m_w, m_w2, m_yn, m_b, m_x, m_p, m_xc, m_tmp;
   DevBuf<double> m_scal;           // 16 * maxB doubles
   DevBuf<int> m_flags;             // 3 * maxB ints
   std::vector<int> last_iters;
@@ -104,7 +106,7 @@ class Context {
   void hx(const double *d_x, double *d_y, int Bw);
   void set_potential_device(double *d_pot);   // distributes d_pot in place
   void lanczos_bounds(double &lo, double &hi);
-  void chfsi_pass(double a, double b, double a0, std::vector<double> &res);
+  void chfsi_pass(double a, double b, double a0, std::vector<double> &res, bool low = false);
   void solve_eigen(double *d_pot, invdft_force_stats *st);
   void density_and_loss(double out4[4]);
   // adjoint

@@ -245,8 +245,8 @@ __global__ void __launch_bounds__(NT) hx_cell_gemm_kernel(FeView fe, const doubl
 // columns each thread loads one double of H_e (a warp reads two contiguous
 // 128-byte column-pair segments) and one double of X_e from shared memory.
 // ---------------------------------------------------------------------------
-template <int NTILE>
-__global__ void __launch_bounds__(NT) hx_cell_dmma_kernel(FeView fe, const double *__restrict__ H,
+template <int NTILE, typename MT>
+__global__ void __launch_bounds__(NT) hx_cell_dmma_kernel(FeView fe, const MT *__restrict__ H,
                                                           const double *__restrict__ x,
                                                           double *__restrict__ Ycell, int B, int mode) {
   extern __shared__ double xs[];  // [kpad][BP] with BP = 8*NTILE, zero padded
@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(NT) hx_cell_dmma_kernel(FeView fe, const doubl
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const double *He = H + e * (int64_t)(ncol >> 1) * 2 * ldh;
+  const MT *He = H + e * (int64_t)(ncol >> 1) * 2 * ldh;
   const int mtiles = (nd + 7) >> 3;
   for (int mt = warp; mt < mtiles; mt += nwarps) {
     const int row = 8 * mt + g;
@@ -273,7 +273,9 @@ __global__ void __launch_bounds__(NT) hx_cell_dmma_kernel(FeView fe, const doubl
     constexpr int U = 8;
     auto load_a = [&](int ks) -> double {
       const int k = 4 * ks + t;
-      return (row_ok && ks < ksteps && k < ncol) ? __ldcs(He + (int64_t)(k >> 1) * 2 * ldh + 2 * row + (k & 1)) : 0.0;
+      return (row_ok && ks < ksteps && k < ncol)
+                 ? (double)__ldcs(He + (int64_t)(k >> 1) * 2 * ldh + 2 * row + (k & 1))
+                 : 0.0;
     };
     double a0[U], a1[U];
 #pragma unroll
@@ -1301,12 +1303,12 @@ void launch_hx_cell_gemm(const FeView &fe, const double *H, const double *x, dou
 }
 
 
-template <int NTILE>
-static void hx_dmma_nt(const FeView &fe, const double *H, const double *x, double *Ycell, int B, int mode,
+template <int NTILE, typename MT>
+static void hx_dmma_nt(const FeView &fe, const MT *H, const double *x, double *Ycell, int B, int mode,
                        cudaStream_t s) {
   static bool attr = false;
   if (!attr) {
-    INVDFT_CUDA(cudaFuncSetAttribute(hx_cell_dmma_kernel<NTILE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_cell_dmma_kernel<NTILE, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      200 * 1024));
     attr = true;
   }
@@ -1314,19 +1316,41 @@ static void hx_dmma_nt(const FeView &fe, const double *H, const double *x, doubl
   const int threads = std::min(NT, 32 * std::max(1, std::min(8, mtiles)));
   const int kpad = 4 * ((fe.nd + 3) / 4);
   const size_t smem = sizeof(double) * (size_t)kpad * 8 * NTILE;
-  hx_cell_dmma_kernel<NTILE><<<(unsigned)fe.nc, threads, smem, s>>>(fe, H, x, Ycell, B, mode);
+  hx_cell_dmma_kernel<NTILE, MT><<<(unsigned)fe.nc, threads, smem, s>>>(fe, H, x, Ycell, B, mode);
   INVDFT_LAUNCH_CHECK();
+}
+
+template <typename MT>
+static void dmma_dispatch(const FeView &fe, const MT *H, const double *x, double *Ycell, int B, int gather_mode,
+                          cudaStream_t s) {
+  if (B <= 8) hx_dmma_nt<1, MT>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 16) hx_dmma_nt<2, MT>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 24) hx_dmma_nt<3, MT>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 32) hx_dmma_nt<4, MT>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 48) hx_dmma_nt<6, MT>(fe, H, x, Ycell, B, gather_mode, s);
+  else if (B <= 64) hx_dmma_nt<8, MT>(fe, H, x, Ycell, B, gather_mode, s);
+  else throw StatusError(5, "block width above 64");
 }
 
 void launch_hx_cell_dmma(const FeView &fe, const double *H, const double *x, double *Ycell, int B,
                          int gather_mode, cudaStream_t s) {
-  if (B <= 8) hx_dmma_nt<1>(fe, H, x, Ycell, B, gather_mode, s);
-  else if (B <= 16) hx_dmma_nt<2>(fe, H, x, Ycell, B, gather_mode, s);
-  else if (B <= 24) hx_dmma_nt<3>(fe, H, x, Ycell, B, gather_mode, s);
-  else if (B <= 32) hx_dmma_nt<4>(fe, H, x, Ycell, B, gather_mode, s);
-  else if (B <= 48) hx_dmma_nt<6>(fe, H, x, Ycell, B, gather_mode, s);
-  else if (B <= 64) hx_dmma_nt<8>(fe, H, x, Ycell, B, gather_mode, s);
-  else throw StatusError(5, "block width above 64");
+  dmma_dispatch<double>(fe, H, x, Ycell, B, gather_mode, s);
+}
+
+void launch_hx_cell_dmma_f32(const FeView &fe, const float *H32, const double *x, double *Ycell, int B,
+                             int gather_mode, cudaStream_t s) {
+  dmma_dispatch<float>(fe, H32, x, Ycell, B, gather_mode, s);
+}
+
+__global__ void narrow_kernel(const double *__restrict__ src, float *__restrict__ dst, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = __double2float_rn(src[i]);
+}
+
+void launch_narrow(const double *src, float *dst, int64_t n, cudaStream_t s) {
+  if (n == 0) return;
+  narrow_kernel<<<ceil_div(n, NT), NT, 0, s>>>(src, dst, n);
+  INVDFT_LAUNCH_CHECK();
 }
 
 template <int BC>

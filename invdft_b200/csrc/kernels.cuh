@@ -48,6 +48,10 @@ void launch_hx_cell_gemm(const FeView &fe, const double *H, const double *x, dou
 // FP64 tensor-core (mma.sync m8n8k4 f64) variant
 void launch_hx_cell_dmma(const FeView &fe, const double *H, const double *x, double *Ycell, int B,
                          int gather_mode, cudaStream_t s);
+// same with cell matrices stored in FP32 (products still accumulated in FP64)
+void launch_hx_cell_dmma_f32(const FeView &fe, const float *H32, const double *x, double *Ycell, int B,
+                             int gather_mode, cudaStream_t s);
+void launch_narrow(const double *src, float *dst, int64_t n, cudaStream_t s);
 // bulk-asynchronous staged variant (persistent CTAs, shared-memory panel ring)
 void launch_hx_cell_gemm_bulk(const FeView &fe, const double *H, const double *x, double *Yslot, int B,
                               int gather_mode, cudaStream_t s);

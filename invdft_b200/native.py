@@ -65,6 +65,7 @@ class Params(C.Structure):
         ("adjoint_max_iter", C.c_int32), ("degeneracy_tol", C.c_double), ("frac_occ_tol", C.c_double),
         ("additional_states", C.c_int32), ("block_size", C.c_int32), ("inter_block_size", C.c_int32),
         ("factor_lda", C.c_double), ("lanczos_steps", C.c_int32), ("precision", C.c_int32),
+        ("mixed_residual_floor", C.c_double),
     ]
 
 
@@ -79,6 +80,7 @@ class Stats(C.Structure):
         ("n_cell_gemm", C.c_int32), ("ms_cell_gemm", C.c_double), ("cell_gemm_bytes", C.c_double),
         ("cell_gemm_flops", C.c_double), ("n_launches", C.c_int64), ("degree", C.c_int32),
         ("upper_bound", C.c_double), ("device_bytes", C.c_double), ("device_bytes_peak", C.c_double),
+        ("passes_low", C.c_int32),
     ]
 
     def as_dict(self) -> dict:

@@ -186,3 +186,19 @@ def test_minres_iteration_cap_returns_finite():
     P, fn, _ = _pair("tiny_h2", adjoint_max_iter=1)
     f, L, st = fn.get_force_vector(P.vxc_init.copy())
     assert np.all(np.isfinite(f)) and st["minres_iters_max"] <= 1
+
+
+@pytest.mark.parametrize("name", ["small_lih"])
+def test_mixed_precision_ladder_reaches_fp64_accuracy(name):
+    """MIXED: filter passes on FP32-stored cell matrices, then FP64 passes; the
+    converged result must match the FP64 oracle (eigenvalues 1e-9 Ha, force 1e-6)."""
+    P, fn, orc = _pair(name, precision=1, mixed_residual_floor=1e-4)
+    pot = P.vxc_init.copy()
+    f_g, L_g, st = fn.get_force_vector(pot.copy())
+    f_o, L_o, ost = orc.get_force_vector(pot.copy())
+    assert st["passes_low"] >= 1
+    assert st["max_residual"] <= 1e-10
+    e, _, _ = fn.eigen()
+    assert np.max(np.abs(e - ost.eigenvalues)) < 1e-9
+    assert abs(L_g - L_o) <= 1e-8 * abs(L_o)
+    assert rel(f_g, f_o) < 1e-6

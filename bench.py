@@ -38,6 +38,28 @@ def _peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+def _fp64_peak_tflops(device) -> float:
+    """FP64 throughput ceiling measured here: cuBLAS DGEMM 8192^3 (2 N^3 flops),
+    best of 5 with CUDA events.  On B200 the FP64 tensor-core rate equals the
+    FP64 FMA-pipe rate, so this bounds any FP64 kernel."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best / 1000.0) / 1e12
+
+
 def _traffic_from_profiles(name: str):
     path = os.path.join(ROOT, "profiles", "cell_gemm_traffic.json")
     try:
@@ -257,9 +279,31 @@ def main():
     n_gemm = sum(s["n_cell_gemm"] for s in stats)
     gemm_ms = sum(s["ms_cell_gemm"] for s in stats)
     gemm_bytes = sum(s["cell_gemm_bytes"] for s in stats)
+    gemm_flops = sum(s["cell_gemm_flops"] for s in stats)
     peaks, pk = _peaks()
-    achieved = gemm_bytes / (gemm_ms / 1000.0) / 1e9 if gemm_ms > 0 else None
-    per_launch_traffic = _traffic_from_profiles(f"{args.config}:{args.precision}")
+    matrix_free = os.environ.get("INVDFT_HX_KERNEL", "sf") == "sf" and P.p <= 7 and args.precision == "fp64"
+    hbm_achieved = gemm_bytes / (gemm_ms / 1000.0) / 1e9 if gemm_ms > 0 else None
+    per_launch_traffic = _traffic_from_profiles(
+        f"{args.config}:{'sf' if matrix_free else 'dmma'}:{args.precision}")
+    if matrix_free:
+        fp64_peak = _fp64_peak_tflops(dev)
+        achieved = gemm_flops / (gemm_ms / 1000.0) / 1e12 if gemm_ms > 0 else None
+        roofline = {"bound": "tensor", "pipe": "fp64 (DFMA; peak = cuBLAS DGEMM measured live, of measured)",
+                    "kernel": "hx_cell_sf (matrix-free FP64 sum-factorised cell products)",
+                    "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                    "frac": (achieved / fp64_peak) if achieved else None, "peak_source": "measured",
+                    "traffic": per_launch_traffic, "launches": n_gemm, "ms_per_launch": gemm_ms / max(n_gemm, 1),
+                    "algorithmic_flops_per_launch": gemm_flops / max(n_gemm, 1),
+                    "algorithmic_bytes_per_launch": gemm_bytes / max(n_gemm, 1),
+                    "hbm_achieved_gbs": hbm_achieved,
+                    "hbm_frac": (hbm_achieved / peaks["hbm_gbs"]) if hbm_achieved else None}
+    else:
+        roofline = {"bound": "hbm", "kernel": "hx_cell_dmma (FP64 cell-matrix x vector block)",
+                    "achieved": hbm_achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": (hbm_achieved / peaks["hbm_gbs"]) if hbm_achieved else None,
+                    "peak_source": pk, "traffic": per_launch_traffic,
+                    "launches": n_gemm, "ms_per_launch": gemm_ms / max(n_gemm, 1),
+                    "algorithmic_bytes_per_launch": gemm_bytes / max(n_gemm, 1)}
     launches = int(sum(s["n_launches"] for s in stats))
     fp64_cmp = None
     if args.precision == "mixed" and not args.no_fp64_compare:
@@ -294,8 +338,8 @@ def main():
                 "workload": f"{args.config}: C2H4-like, FE order {P.p}, {P.n_nodes} DoF, {P.n_cells} cells, "
                             f"{P.n_states} states, {P.n_child_cells} v_xc cells / {P.n_child_nodes} nodes, "
                             f"precision {args.precision}",
-                "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (cell matrices "
-                f"{P.n_cells * P.nd * P.nd * 8 / 1e9:.2f} GB)",
+                "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (state block + cell results "
+                f"{(P.n_nodes + P.n_cells * P.nd) * P.n_states * 8 / 1e9:.2f} GB per HX)",
                 "step": "one getForceVector at a new v_xc on the path guess -> v_xc*",
                 "chebyshev_passes": [s["passes"] for s in stats],
                 "chebyshev_passes_fp32_stored": [s["passes_low"] for s in stats],
@@ -304,16 +348,14 @@ def main():
                 "spectrum_upper_bound": stats[-1]["upper_bound"],
                 "minres_iters_max": [s["minres_iters_max"] for s in stats],
                 "hx_columns": [s["n_hx_columns"] for s in stats],
+                "stage_ms_mean": {k: float(np.mean([s[f"ms_{k}"] for s in stats]))
+                                  for k in ("eigen", "density", "adjoint", "transfer")},
+                "hx_kernel": "matrix-free sum factorisation" if matrix_free else "stored cell matrices (DMMA)",
                 "loss": [s["loss"] for s in stats], **info},
             "e2e": {"value": e2e, "unit": "force-evals/s", "h2d_bytes_per_step": 8 * P.n_child_nodes,
                     "d2h_bytes_per_step": 8 * P.n_child_nodes + 8},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": "hx_cell_gemm (FP64 cell-matrix x vector block)",
-                         "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
-                         "peak_source": pk, "traffic": per_launch_traffic,
-                         "launches": n_gemm, "ms_per_launch": gemm_ms / max(n_gemm, 1),
-                         "algorithmic_bytes_per_launch": gemm_bytes / max(n_gemm, 1)},
+            "roofline": roofline,
             "cpu_baseline": dict(value=cpu_v, unit="force-evals/s", **cpu_meta),
             "clocks": clk.summary(),
         }

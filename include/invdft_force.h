@@ -202,7 +202,7 @@ invdft_status invdft_set_potential(invdft_ctx *ctx, const double *pot);
 
 /* Lowdin HX on device blocks: d_y = M^-1/2 C^T sum_e H_e (C M^-1/2 d_x)_e
  * (KohnShamDFTBaseOperator::HXWithLowdinOrthonormalisedInput as called at
- * MultiVectorAdjointLinearSolverProblem.cpp:1353). */
+ * MultiVectorAdjointLinearSolverProblem.cpp:1353).  B in [1, 64]. */
 invdft_status invdft_hx(invdft_ctx *ctx, const double *d_x, double *d_y, int32_t B);
 
 /* MultiVectorAdjointLinearSolverProblem::updateInputPsi (:818-910).

@@ -194,7 +194,7 @@ invdft_status invdft_set_potential(invdft_ctx *ctx, const double *pot) {
 
 invdft_status invdft_hx(invdft_ctx *ctx, const double *d_x, double *d_y, int32_t B) {
   return guard(ctx, [&](invdft::Context &c) {
-    if (!d_x || !d_y || B < 1 || B > c.N) throw invdft::StatusError(INVDFT_BAD_ARG, "bad hx arguments");
+    if (!d_x || !d_y || B < 1 || B > 64) throw invdft::StatusError(INVDFT_BAD_ARG, "bad hx arguments (B in [1, 64])");
     c.hx(d_x, d_y, B);
     c.check_device_error();
   });

@@ -242,6 +242,17 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
                               M1[a * n1 + ap] * M1[b * n1 + bp] * S1[c * n1 + cp];
     }
   }
+  // matrix-free variant: phi, the Gauss-point collocation derivative, 1D weights
+  if (n1 <= kSfMaxN) {
+    for (int q = 0; q < n1; ++q) {
+      auto dv = lagrange_deriv(gp, gp[q]);
+      for (int a = 0; a < n1; ++a) {
+        sfm.phi[q * n1 + a] = ph[(size_t)q * n1 + a];
+        sfm.dq[q * n1 + a] = dv[a];
+      }
+      sfm.w[q] = gq[q];
+    }
+  }
   std::vector<double> w3(nd);
   for (int i = 0; i < nd; ++i) w3[i] = gw[i % n1] * gw[(i / n1) % n1] * gw[i / (n1 * n1)];
 
@@ -302,6 +313,10 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   upload_cons(cchild, d->cons_child, ncn, s);
   cons_gw.upload(cgw, s);
   d_slot_of.upload(slot_of, s);
+  // eight entries of padding: the pipelined assembly copies slot ranges in
+  // 16-byte units and may read up to three entries past the last node
+  dptr_h.resize(dptr_h.size() + 8, dptr_h.back());
+  hptr_h.resize(hptr_h.size() + 8, hptr_h.back());
   d_dptr.upload(dptr_h, s);
   d_hptr.upload(hptr_h, s);
   d_hslot.upload(hslot_h, s);
@@ -357,13 +372,17 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   fe.cons_rows = cpsi.rows.p; fe.ncons = cpsi.n;
   fe.slot_of = d_slot_of.p; fe.dptr = d_dptr.p; fe.hptr = d_hptr.p; fe.hslot = d_hslot.p; fe.hw = d_hw.p;
   fe.zptr = d_zptr.p; fe.nhang = nhang; fe.z = d_z.p;
+  d_hvg.alloc((size_t)std::max(cpsi.n, 1) * 64);
+  fe.hvg = d_hvg.p;
   fe.err = d_err.p;
   {
-    // register-blocked row-stream kernel by default; INVDFT_HX_KERNEL=bulk selects
-    // the bulk-asynchronous staged variant
+    // matrix-free cell products by default (FE orders up to 7); INVDFT_HX_KERNEL
+    // = dmma | rowstream | bulk selects a variant on stored cell matrices
     const char *v = std::getenv("INVDFT_HX_KERNEL");
-    const std::string k = v ? v : "dmma";
-    hx_variant = k == "bulk" ? 2 : (k == "rowstream" ? 1 : 0);
+    const std::string k = v ? v : (n1 <= kSfMaxN ? "sf" : "dmma");
+    hx_variant = k == "bulk" ? 2 : (k == "rowstream" ? 1 : (k == "sf" && n1 <= kSfMaxN ? 3 : 0));
+    const char *t = std::getenv("INVDFT_SF_TUNE");
+    sf_tune = t ? std::atoi(t) : (n1 <= 6 ? 1 : 0);   // two CTAs per SM where registers allow
   }
   fe.inv_sqrt_mass = invsqrtM.p; fe.sqrt_mass = sqrtM.p;
   cv.ncc = ncc; cv.nchild_nodes = ncn; cv.cell_nodes = ch_nodes.p; cv.jxw = ch_jxw.p; cv.parent = ch_parent.p;
@@ -408,13 +427,13 @@ void Context::set_params(const invdft_params *pp) {
 
 void Context::alloc_state() {
   const int maxB = N;
-  H.alloc((size_t)nc * ((nd + 1) / 2) * 2 * ldh);
   X.alloc((size_t)nn * N);
   Yb.alloc((size_t)nn * N);
   Zb.alloc((size_t)nn * N);
   Wb.alloc((size_t)nn * N);
-  Ycell.alloc((size_t)nc * nd * std::max(maxB, 2));
+  Ycell.alloc((size_t)nc * nd * std::max(maxB, 2) + 2);   // +2: 16-byte rounded segment copies
   vks.alloc(nc * nq);
+  if (hx_variant == 3) vj.alloc(nc * nq);
   rho.alloc(nc * nq);
   u.alloc(nc * nq);
   psi.alloc((size_t)nn * N);
@@ -454,15 +473,23 @@ void Context::cell_gemm(const double *d_x, int Bw, bool low) {
   const bool rec = profile && ev_used + 2 <= (int)ev_pool.size();
   if (rec) INVDFT_CUDA(cudaEventRecord(ev_pool[ev_used], stream));
   if (low) launch_hx_cell_dmma_f32(fe, H32.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
+  else if (hx_variant == 3) launch_hx_cell_sf(fe, sfm, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, sf_tune, stream);
   else if (hx_variant == 0) launch_hx_cell_dmma(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
   else if (hx_variant == 2) launch_hx_cell_gemm_bulk(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
   else launch_hx_cell_gemm(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
   if (rec) {
     INVDFT_CUDA(cudaEventRecord(ev_pool[ev_used + 1], stream));
     ev_used += 2;
-    // algorithmic traffic: cell matrices once, the block once, the cell results once
-    prof_bytes += (low ? 4.0 : 8.0) * (double)nc * nd * nd + 8.0 * ((double)nn * Bw + (double)nc * nd * Bw);
-    prof_flops += 2.0 * (double)nc * nd * nd * Bw;
+    if (!low && hx_variant == 3) {
+      // algorithmic traffic: the block once, v JxW once, the cell results once;
+      // 12 n1^4 FMAs per (cell, column)
+      prof_bytes += 8.0 * ((double)nn * Bw + (double)nc * nq + (double)nc * nd * Bw);
+      prof_flops += 24.0 * (double)nc * nd * n1 * Bw;
+    } else {
+      // algorithmic traffic: cell matrices once, the block once, the cell results once
+      prof_bytes += (low ? 4.0 : 8.0) * (double)nc * nd * nd + 8.0 * ((double)nn * Bw + (double)nc * nd * Bw);
+      prof_flops += 2.0 * (double)nc * nd * nd * Bw;
+    }
   }
 }
 
@@ -492,6 +519,7 @@ void Context::profile_end(invdft_force_stats *st) {
 
 void Context::hx(const double *d_x, double *d_y, int Bw) {
   if (!have_H) throw StatusError(INVDFT_NOT_READY, "no potential set");
+  Ycell.ensure((size_t)nc * nd * Bw + 2);
   cell_gemm(d_x, Bw);
   AsmEpilogue epi;
   epi.kind = AsmEpilogue::STORE;
@@ -500,10 +528,22 @@ void Context::hx(const double *d_x, double *d_y, int Bw) {
   n_hx_cols += Bw;
 }
 
+// Stored cell matrices back every variant but the matrix-free one, and the
+// FP32-stored filter of the mixed-precision ladder.
+bool Context::needs_cell_matrices() const {
+  return hx_variant != 3 || prm.precision == INVDFT_PRECISION_MIXED;
+}
+
 void Context::set_potential_device(double *d_pot) {
   launch_distribute(cchild.rows.p, cchild.ptr.p, cchild.masters.p, cchild.w.p, cchild.n, d_pot, 1, stream);
   launch_child_to_parent_quad(cv, d_pot, v_base.p, v_lda.p, prm.factor_lda, vks.p, nc * nq, stream);
-  launch_build_cell_h(fe, vks.p, jxw.p, Kref.p, H.p, stream);
+  if (hx_variant == 3) launch_mul(vks.p, jxw.p, vj.p, nc * nq, stream);
+  if (needs_cell_matrices()) {
+    H.ensure((size_t)nc * ((nd + 1) / 2) * 2 * ldh);
+    launch_build_cell_h(fe, vks.p, jxw.p, Kref.p, H.p, stream);
+  } else {
+    H.release();
+  }
   have_H = true;
   have_H32 = false;
   if (prm.precision == INVDFT_PRECISION_MIXED) {

@@ -48,7 +48,14 @@ class Context {
   int nhang = 0;
   DevBuf<double> d_hw;
   int ldh = 0;
-  int hx_variant = 0;   // 0: FP64 tensor core (mma.sync f64), 1: row-stream DFMA, 2: bulk-staged DFMA
+  // cell products: 3 matrix-free sum factorisation (default), 0 FP64 tensor core
+  // on stored cell matrices (mma.sync f64), 1 row-stream DFMA, 2 bulk-staged DFMA
+  int hx_variant = 3;
+  int sf_tune = 0;                 // launch shape of the matrix-free kernel
+  SfMats sfm{};                    // reference-element matrices of the matrix-free variant
+  DevBuf<double> vj;               // [nc][nq] v_KS * JxW (matrix-free variant)
+  DevBuf<double> d_hvg;            // [ncons][64] pre-gathered constrained rows (matrix-free variant)
+  bool needs_cell_matrices() const;
   void check_device_error();
   DevBuf<double> sqrtM, invsqrtM, diagA, diagSqrtA;
   std::vector<char> h_free;        // unconstrained psi rows

@@ -7,6 +7,8 @@
 #include "kernels.cuh"
 
 #include <algorithm>
+#include <cstdlib>
+#include <string>
 #include <atomic>
 
 namespace invdft {
@@ -315,6 +317,169 @@ __global__ void __launch_bounds__(NT) hx_cell_dmma_kernel(FeView fe, const MT *_
 }
 
 // ---------------------------------------------------------------------------
+// HX, part 1, matrix-free variant: Y_e = H_e X_e by sum factorisation, never
+// forming H_e.  With u the cell values on the GLL nodes, Gauss-point values
+// uq = (phi (x) phi (x) phi) u, collocation derivatives g_d = Dq_d uq, and
+// per-point weights, H_e u = phi3^T (vJ uq) + 1/2 h sum_d phi3^T Dq_d^T (W3 g_d),
+// which equals (1/2 h K_ref + N^T diag(v JxW) N) u in exact arithmetic (the
+// (p+1)-point Gauss rule integrates every product in the stiffness exactly).
+// 12 N^4 FMAs per (cell, column) instead of 2 N^6, and no cell-matrix traffic:
+// the kernel is bound by the FP64 pipes and shared memory, not by HBM.
+//
+// A CTA holds 16 (cell, column) pairs: C columns of 16/C consecutive cells.
+// Shared arrays are [point][pair], so a warp (16 pairs x 2 tensor lines)
+// touches two 128-byte rows per access, free of bank conflicts.  Thread
+// (pair p, line L) owns tensor line L in every stage; the direction of the
+// line changes between stages.
+// ---------------------------------------------------------------------------
+template <int N, int DIR>
+__device__ __forceinline__ int sf_point(int L, int k) {
+  if (DIR == 0) return k + N * L;                              // x-line, L = j + N k
+  if (DIR == 1) return (L % N) + N * k + N * N * (L / N);      // y-line, L = i + N k
+  return L + N * N * k;                                        // z-line, L = i + N j
+}
+
+template <int N, int DIR>
+__device__ __forceinline__ void sf_load(const double *a, int L, int p, double (&r)[N]) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) r[k] = a[sf_point<N, DIR>(L, k) * 16 + p];
+}
+template <int N, int DIR>
+__device__ __forceinline__ void sf_store(double *a, int L, int p, const double (&r)[N]) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) a[sf_point<N, DIR>(L, k) * 16 + p] = r[k];
+}
+// out[q] = sum_a M[q][a] in[a]  (M row-major N x N)
+template <int N>
+__device__ __forceinline__ void sf_apply(const double *M, const double (&in)[N], double (&out)[N]) {
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    double s = 0.0;
+#pragma unroll
+    for (int a = 0; a < N; ++a) s = fma(M[q * N + a], in[a], s);
+    out[q] = s;
+  }
+}
+// out[a] += sum_q M[q][a] in[q]
+template <int N>
+__device__ __forceinline__ void sf_apply_t(const double *M, const double (&in)[N], double (&out)[N]) {
+#pragma unroll
+  for (int a = 0; a < N; ++a) {
+    double s = out[a];
+#pragma unroll
+    for (int q = 0; q < N; ++q) s = fma(M[q * N + a], in[q], s);
+    out[a] = s;
+  }
+}
+
+template <int N, int MINB>
+__global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe, SfMats mt, const double *__restrict__ vj,
+                                                                const double *__restrict__ x,
+                                                                double *__restrict__ Ycell, int B, int C, int mode) {
+  constexpr int N2 = N * N, N3 = N2 * N;
+  extern __shared__ double sm[];
+  double *A = sm, *Bs = sm + N3 * 16, *Cs = sm + 2 * N3 * 16;
+  const int p = threadIdx.x & 15, L = threadIdx.x >> 4;
+  const int G = 16 / C;
+  const int g = p / C, c = p - g * C;
+  const int64_t e = (int64_t)blockIdx.x * G + g;
+  const int b = blockIdx.y * C + c;
+  const bool act = e < fe.nc && b < B;
+  const double hh = act ? 0.5 * fe.cell_h[e] : 0.0;
+  double wa = 0.0, wb = 0.0;   // weights of the two coordinates off the line (compile-time indices)
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    if (L % N == k) wa = mt.w[k];
+    if (L / N == k) wb = mt.w[k];
+  }
+  const double f = hh * wa * wb;
+  double r[N], s[N], gx[N];
+  // gather of the z-line L straight into registers: all N node indices, then
+  // all 2N independent value loads, then the (rare) hanging rows; phi along z
+  {
+    int m[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      const int l = L + N2 * k;
+      m[k] = act ? (mode == GATHER_PLAIN ? fe.cell_nodes[e * N3 + l] : fe.cell_map[e * N3 + l]) : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      const bool direct = act && m[k] >= 0;
+      const double xv = direct ? x[(int64_t)m[k] * B + b] : 0.0;
+      const double sc = (direct && mode != GATHER_PLAIN) ? fe.inv_sqrt_mass[m[k]] : 1.0;
+      r[k] = xv * sc;
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k)   // constrained rows: pre-gathered by hanging_gather_kernel
+      if (act && m[k] < 0) r[k] = fe.hvg[(int64_t)(-m[k] - 1) * B + b];
+  }
+  sf_apply<N>(mt.phi, r, s);
+  sf_store<N, 2>(A, L, p, s);
+  __syncthreads();
+  sf_load<N, 1>(A, L, p, r);             // phi along y
+  sf_apply<N>(mt.phi, r, s);
+  sf_store<N, 1>(Bs, L, p, s);
+  __syncthreads();
+  sf_load<N, 0>(Bs, L, p, r);            // phi along x: Gauss-point values, then d/dx
+  sf_apply<N>(mt.phi, r, s);
+  sf_store<N, 0>(A, L, p, s);
+  sf_apply<N>(mt.dq, s, gx);
+#pragma unroll
+  for (int q = 0; q < N; ++q) gx[q] *= f * mt.w[q];
+  __syncthreads();
+  sf_load<N, 1>(A, L, p, r);             // d/dy, weighted, kept for the y back pass
+  sf_apply<N>(mt.dq, r, s);
+#pragma unroll
+  for (int q = 0; q < N; ++q) s[q] *= f * mt.w[q];
+  sf_store<N, 1>(Cs, L, p, s);
+  {
+    double v[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] = act ? vj[e * N3 + L + N2 * k] : 0.0;
+    sf_load<N, 2>(A, L, p, r);           // d/dz, the z back pass and the potential term
+    sf_apply<N>(mt.dq, r, s);
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      s[q] *= f * mt.w[q];
+      r[q] *= v[q];
+    }
+    sf_apply_t<N>(mt.dq, s, r);
+    sf_store<N, 2>(Bs, L, p, r);
+  }
+  __syncthreads();
+  sf_load<N, 1>(Bs, L, p, r);            // y back pass of the derivative term
+  sf_load<N, 1>(Cs, L, p, s);
+  sf_apply_t<N>(mt.dq, s, r);
+  sf_store<N, 1>(A, L, p, r);
+  __syncthreads();
+  sf_load<N, 0>(A, L, p, r);             // x back pass, then phi^T along x
+  sf_apply_t<N>(mt.dq, gx, r);
+#pragma unroll
+  for (int a = 0; a < N; ++a) s[a] = 0.0;
+  sf_apply_t<N>(mt.phi, r, s);
+  sf_store<N, 0>(Bs, L, p, s);
+  __syncthreads();
+  sf_load<N, 1>(Bs, L, p, r);            // phi^T along y
+#pragma unroll
+  for (int a = 0; a < N; ++a) s[a] = 0.0;
+  sf_apply_t<N>(mt.phi, r, s);
+  sf_store<N, 1>(A, L, p, s);
+  __syncthreads();
+  sf_load<N, 2>(A, L, p, r);             // phi^T along z, straight to the cell-result slots
+#pragma unroll
+  for (int a = 0; a < N; ++a) s[a] = 0.0;
+  sf_apply_t<N>(mt.phi, r, s);
+  if (act) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      const int sl = fe.slot_of[e * N3 + L + N2 * k];
+      if (sl >= 0) Ycell[(int64_t)sl * B + b] = s[k];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // HX, part 1, bulk-asynchronous variant.  Persistent CTAs walk their cells;
 // thread 0 streams contiguous column panels of H_e (PW columns x ldh doubles)
 // with cp.async.bulk into an S-stage shared-memory ring completed through
@@ -546,6 +711,7 @@ __global__ void __launch_bounds__(NT) hx_assemble_tile_kernel(FeView fe, const d
   int *hp = dp + TR + 1;
   __shared__ double red[NT];
   const int64_t r0 = (int64_t)blockIdx.x * TR;
+  if (r0 >= fe.nnodes) return;   // grid sized by the caller: never past the last node
   const int rows = (int)min((int64_t)TR, fe.nnodes - r0);
   const bool need_in = epi.kind == AsmEpilogue::CHEB || epi.kind == AsmEpilogue::VMULT ||
                        epi.kind == AsmEpilogue::MINRES;
@@ -653,6 +819,193 @@ __global__ void __launch_bounds__(NT) hx_assemble_tile_kernel(FeView fe, const d
     }
   }
   if (epi.kind == AsmEpilogue::MINRES) {
+    red[threadIdx.x] = dot;
+    __syncthreads();
+    if (threadIdx.x < B) {
+      double sum = 0.0;
+      for (int q = 0; q < RR; ++q) sum += red[q * B + threadIdx.x];
+      epi.dot_partial[(int64_t)blockIdx.x * B + threadIdx.x] = sum;
+    }
+  }
+}
+
+// One tile of the assembly: node rows r0 .. r0+rows-1 with their direct slots
+// read from segp[sl*B + j - a0] (a shared-memory copy of the tile's slot
+// segment, or the cell results themselves with a0 = 0), their slot and
+// hanging ranges from dp/hp, M^-1/2 from ism and the epilogue inputs from
+// t_in/t_prev (tile-local, row stride B).  Thread (rr, j) handles column j of
+// rows rr, rr+RR, ... in a fixed order.
+__device__ __forceinline__ void assemble_tile_rows(const FeView &fe, const double *segp, int64_t a0,
+                                                   const int *dp, const int *hp, const double *ism,
+                                                   const double *t_in, const double *t_prev, int64_t r0, int rows,
+                                                   double *__restrict__ out, int B, const AsmEpilogue &epi,
+                                                   double &dot) {
+  const int RR = NT / B;
+  const int j = threadIdx.x % B, rr = threadIdx.x / B;
+  if (rr >= RR) return;
+  for (int lr = rr; lr < rows; lr += RR) {
+    const int64_t n = r0 + lr;
+    const int d0 = dp[lr], d1 = dp[lr + 1];
+    double acc = 0.0;
+    for (int sl = d0; sl < d1; ++sl) acc += segp[(int64_t)sl * B + j - a0];
+    const int k1 = hp[lr + 1];
+    for (int k = hp[lr]; k < k1; ++k) acc += fe.hw[k] * fe.z[(int64_t)fe.hslot[k] * B + j];
+    acc *= ism[lr];
+    const int64_t idx = n * B + j;
+    const int li = lr * B + j;
+    switch (epi.kind) {
+      case AsmEpilogue::STORE: out[idx] = acc; break;
+      case AsmEpilogue::CHEB: {
+        double v = epi.alpha * (acc - epi.c * t_in[li]);
+        if (epi.prev) v -= epi.beta * t_prev[li];
+        out[idx] = v;
+        break;
+      }
+      case AsmEpilogue::VMULT: out[idx] = acc - epi.eps[j] * t_in[li]; break;
+      case AsmEpilogue::RHS: {
+        double v = 0.0;
+        if (d1 > d0 && ism[lr] != 0.0) {
+          double mu = 0.0;
+          for (int k = 0; k < B; ++k) mu = fma(epi.Mu[k * B + j], epi.psi[n * B + k], mu);
+          v = epi.occ4[j] * acc - 2.0 * fe.sqrt_mass[n] * mu;
+        }
+        out[idx] = v;
+        break;
+      }
+      case AsmEpilogue::MINRES: {
+        const double vv = t_in[li];
+        const double yn = acc - epi.eps[j] * vv - epi.minres_coef[j] * t_prev[li];
+        out[idx] = yn;
+        dot = fma(vv, yn, dot);
+        break;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// HX, part 2, bulk-pipelined: persistent CTAs walk the full tiles of TR nodes
+// (tile blockIdx.x + i*gridDim.x).  Everything a tile reads is contiguous in
+// HBM -- its slot and hanging ranges, M^-1/2, the epilogue inputs and its
+// slot segment of the cell results -- so thread 0 streams tile i+1 into the
+// other of two shared-memory stages with cp.async.bulk (one mbarrier per
+// stage) while the CTA reduces tile i.  The slot segment is copied from its
+// 16-byte-aligned start (offset a0 kept in shared memory); a segment longer
+// than the stage holds is read from HBM directly.  Waits are bounded and
+// voted across the CTA: a wait that gives up sets fe.err, thread 0 drains
+// the other stage (bounded again) and the CTA returns.  The last, partial
+// tile is reduced with direct loads by one CTA after the loop.
+// ---------------------------------------------------------------------------
+struct AsmStage {
+  double *seg, *in, *prev, *ism;
+  int *dp, *hp;
+};
+
+__device__ __forceinline__ AsmStage asm_stage(unsigned char *base, int st, int TR, int cap, int B) {
+  const size_t seg_n = (size_t)cap * B + 2, blk = (size_t)TR * B;
+  const size_t stage_bytes = 8 * (seg_n + 2 * blk + TR) + 4 * 2 * ((size_t)TR + 4);
+  double *p = reinterpret_cast<double *>(base + (size_t)st * ((stage_bytes + 127) & ~(size_t)127));
+  AsmStage s;
+  s.seg = p;
+  s.in = p + seg_n;
+  s.prev = s.in + blk;
+  s.ism = s.prev + blk;
+  s.dp = reinterpret_cast<int *>(s.ism + TR);
+  s.hp = s.dp + TR + 4;
+  return s;
+}
+
+__global__ void __launch_bounds__(NT) hx_assemble_bulk_kernel(FeView fe, const double *__restrict__ Ycell,
+                                                              double *__restrict__ out, int B, AsmEpilogue epi,
+                                                              int TR, int cap) {
+  extern __shared__ __align__(128) unsigned char sm_ab[];
+  __shared__ uint64_t bars[2];
+  __shared__ double red[NT];
+  const int64_t nfull = fe.nnodes / TR;
+  const int64_t G = gridDim.x;
+  const int64_t cnt = blockIdx.x < nfull ? (nfull - 1 - blockIdx.x) / G + 1 : 0;
+  const bool need_in = epi.kind == AsmEpilogue::CHEB || epi.kind == AsmEpilogue::VMULT ||
+                       epi.kind == AsmEpilogue::MINRES;
+  const bool need_prev = (epi.kind == AsmEpilogue::CHEB && epi.prev) || epi.kind == AsmEpilogue::MINRES;
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // thread 0: stream tile i (slot bounds s0, s1 already loaded) into stage i & 1
+  auto issue = [&](int64_t i, int s0, int s1) {
+    const int64_t r0 = (blockIdx.x + i * G) * TR;
+    AsmStage S = asm_stage(sm_ab, (int)(i & 1), TR, cap, B);
+    uint64_t *bar = &bars[i & 1];
+    uint32_t bytes = 2u * 4u * (uint32_t)(TR + 4) + 8u * (uint32_t)TR;
+    if (need_in) bytes += 8u * (uint32_t)TR * B;
+    if (need_prev) bytes += 8u * (uint32_t)TR * B;
+    const bool staged = s1 - s0 <= cap;
+    const int64_t a0 = ((int64_t)s0 * B) & ~(int64_t)1, a1 = ((int64_t)s1 * B + 1) & ~(int64_t)1;
+    if (staged) bytes += 8u * (uint32_t)(a1 - a0);
+    mbar_expect_tx(bar, bytes);
+    bulk_g2s(S.dp, fe.dptr + r0, 4u * (TR + 4), bar);
+    bulk_g2s(S.hp, fe.hptr + r0, 4u * (TR + 4), bar);
+    bulk_g2s(S.ism, fe.inv_sqrt_mass + r0, 8u * TR, bar);
+    if (need_in) bulk_g2s(S.in, epi.in + r0 * B, 8u * TR * B, bar);
+    if (need_prev) bulk_g2s(S.prev, epi.prev + r0 * B, 8u * TR * B, bar);
+    if (staged && a1 > a0) bulk_g2s(S.seg, Ycell + a0, 8u * (uint32_t)(a1 - a0), bar);
+  };
+  auto bounds = [&](int64_t i, int &s0, int &s1) {
+    const int64_t r0 = (blockIdx.x + i * G) * TR;
+    s0 = fe.dptr[r0];
+    s1 = fe.dptr[r0 + TR];
+  };
+  int pre0 = 0, pre1 = 0;   // thread 0: slot bounds of tile i+2
+  if (threadIdx.x == 0) {
+    int s0, s1;
+    if (cnt > 0) { bounds(0, s0, s1); issue(0, s0, s1); }
+    if (cnt > 1) { bounds(1, s0, s1); issue(1, s0, s1); }
+  }
+  double dot = 0.0;
+  for (int64_t i = 0; i < cnt; ++i) {
+    if (threadIdx.x == 0 && i + 2 < cnt) bounds(i + 2, pre0, pre1);   // in flight during this tile
+    bool ok = true;
+    {
+      long long it = 0;
+      while (!mbar_try_wait(&bars[i & 1], (uint32_t)((i >> 1) & 1))) {
+        if (++it > kWaitLimit) { ok = false; break; }
+      }
+    }
+    if (!__syncthreads_and(ok)) {
+      if (threadIdx.x == 0) {
+        atomicExch(fe.err, 1);
+        if (i + 1 < cnt) {   // drain the other stage's copies before the CTA leaves
+          long long it = 0;
+          while (!mbar_try_wait(&bars[(i + 1) & 1], (uint32_t)(((i + 1) >> 1) & 1)) && ++it <= kWaitLimit) {
+          }
+        }
+      }
+      return;
+    }
+    const int64_t r0 = (blockIdx.x + i * G) * TR;
+    AsmStage S = asm_stage(sm_ab, (int)(i & 1), TR, cap, B);
+    const int s0 = S.dp[0], s1 = S.dp[TR];
+    const bool staged = s1 - s0 <= cap;
+    const int64_t a0 = staged ? (((int64_t)s0 * B) & ~(int64_t)1) : 0;
+    assemble_tile_rows(fe, staged ? S.seg : Ycell, a0, S.dp, S.hp, S.ism, S.in, S.prev, r0, TR, out, B, epi, dot);
+    __syncthreads();
+    if (threadIdx.x == 0 && i + 2 < cnt) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(i + 2, pre0, pre1);
+    }
+  }
+  // the partial last tile, direct loads, on the CTA next in the round robin
+  const int64_t rt = nfull * TR;
+  if (rt < fe.nnodes && blockIdx.x == nfull % G) {
+    const int rows = (int)(fe.nnodes - rt);
+    assemble_tile_rows(fe, Ycell, 0, fe.dptr + rt, fe.hptr + rt, fe.inv_sqrt_mass + rt,
+                       need_in ? epi.in + rt * B : nullptr, need_prev ? epi.prev + rt * B : nullptr, rt, rows,
+                       out, B, epi, dot);
+  }
+  if (epi.kind == AsmEpilogue::MINRES) {
+    const int RR = NT / B;
     red[threadIdx.x] = dot;
     __syncthreads();
     if (threadIdx.x < B) {
@@ -1342,6 +1695,83 @@ void launch_hx_cell_dmma_f32(const FeView &fe, const float *H32, const double *x
   dmma_dispatch<float>(fe, H32, x, Ycell, B, gather_mode, s);
 }
 
+// hvg[r][b] = sum_t gw_t x[master_t][b] for every constrained row r: the
+// Lowdin gather of the hanging (and Dirichlet) rows, in the same FMA order as
+// gather_value, so the matrix-free kernel reads them with one load each
+__global__ void hanging_gather_kernel(FeView fe, const double *__restrict__ x, int B) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)fe.ncons * B) return;
+  const int r = (int)(idx / B), b = (int)(idx - (int64_t)r * B);
+  double v = 0.0;
+  for (int t = fe.cons_ptr[r]; t < fe.cons_ptr[r + 1]; ++t)
+    v = fma(fe.cons_gw[t], x[(int64_t)fe.cons_masters[t] * B + b], v);
+  fe.hvg[idx] = v;
+}
+
+template <int N, int MINB>
+static void hx_sf_n(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell, int B,
+                    int mode, cudaStream_t s) {
+  constexpr int threads = 16 * N * N;
+  const size_t smem = sizeof(double) * 3 * (size_t)N * N * N * 16;
+  static bool attr = false;
+  if (!attr) {
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_cell_sf_kernel<N, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    attr = true;
+  }
+  // C columns of 16/C cells per CTA; C = the smallest power of two >= B, at most 16
+  int C = 1;
+  while (C < B && C < 16) C <<= 1;
+  const int G = 16 / C;
+  const dim3 grid((unsigned)((fe.nc + G - 1) / G), (unsigned)((B + C - 1) / C));
+  hx_cell_sf_kernel<N, MINB><<<grid, threads, smem, s>>>(fe, mt, vj, x, Ycell, B, C, mode);
+  INVDFT_LAUNCH_CHECK();
+}
+
+template <int MINB>
+static void hx_sf_dispatch(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell,
+                           int B, int mode, cudaStream_t s) {
+  switch (fe.n1) {
+    case 2: hx_sf_n<2, MINB>(fe, mt, vj, x, Ycell, B, mode, s); break;
+    case 3: hx_sf_n<3, MINB>(fe, mt, vj, x, Ycell, B, mode, s); break;
+    case 4: hx_sf_n<4, MINB>(fe, mt, vj, x, Ycell, B, mode, s); break;
+    case 5: hx_sf_n<5, MINB>(fe, mt, vj, x, Ycell, B, mode, s); break;
+    case 6: hx_sf_n<6, MINB>(fe, mt, vj, x, Ycell, B, mode, s); break;
+    case 7: if (MINB == 1) { hx_sf_n<7, 1>(fe, mt, vj, x, Ycell, B, mode, s); break; }
+      [[fallthrough]];
+    default: throw StatusError(5, "matrix-free HX: FE order outside the compiled launch shapes");
+  }
+}
+
+void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell,
+                       int B, int gather_mode, int tune, cudaStream_t s) {
+  if (gather_mode != GATHER_PLAIN && fe.ncons > 0) {
+    hanging_gather_kernel<<<ceil_div((int64_t)fe.ncons * B, NT), NT, 0, s>>>(fe, x, B);
+    INVDFT_LAUNCH_CHECK();
+  }
+  if (tune == 1 && fe.n1 <= 6) {
+    hx_sf_dispatch<2>(fe, mt, vj, x, Ycell, B, gather_mode, s);
+    return;
+  }
+  if (fe.n1 == 8) {
+    hx_sf_n<8, 1>(fe, mt, vj, x, Ycell, B, gather_mode, s);
+    return;
+  }
+  hx_sf_dispatch<1>(fe, mt, vj, x, Ycell, B, gather_mode, s);
+}
+
+__global__ void mul_kernel(const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ out,
+                           int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a[i] * b[i];
+}
+
+void launch_mul(const double *a, const double *b, double *out, int64_t n, cudaStream_t s) {
+  if (n == 0) return;
+  mul_kernel<<<ceil_div(n, NT), NT, 0, s>>>(a, b, out, n);
+  INVDFT_LAUNCH_CHECK();
+}
+
 __global__ void narrow_kernel(const double *__restrict__ src, float *__restrict__ dst, int64_t n) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) dst[i] = __double2float_rn(src[i]);
@@ -1397,10 +1827,46 @@ static void assemble_shape(int B, int &TR, int &cap) {
   cap = 2 * TR;   // ~1.6 slots per node on average
 }
 
+// launch shape of the bulk-pipelined assembly: TR nodes per tile (a multiple
+// of 4), 2 TR slots per stage, two stages; persistent grid of as many CTAs as
+// fit on the SMs, at most one per full tile
+struct AsmBulkShape {
+  int TR, cap, grid;
+  size_t smem;
+};
+static AsmBulkShape asm_bulk_shape(const FeView &fe, int B) {
+  AsmBulkShape sh;
+  sh.TR = std::max(16, std::min(256, 1024 / B)) & ~3;
+  sh.cap = 2 * sh.TR;
+  const size_t seg_n = (size_t)sh.cap * B + 2, blk = (size_t)sh.TR * B;
+  const size_t stage = 8 * (seg_n + 2 * blk + sh.TR) + 4 * 2 * ((size_t)sh.TR + 4);
+  sh.smem = 2 * ((stage + 127) & ~(size_t)127);
+  static int nsm = 0;
+  static int occ[257] = {};
+  if (!nsm) {
+    int dev = 0;
+    INVDFT_CUDA(cudaGetDevice(&dev));
+    INVDFT_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_assemble_bulk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     200 * 1024));
+  }
+  if (!occ[B]) {
+    int o = 0;
+    INVDFT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, hx_assemble_bulk_kernel, NT, sh.smem));
+    occ[B] = std::max(o, 1);
+  }
+  const int64_t nfull = fe.nnodes / sh.TR;
+  sh.grid = (int)std::max<int64_t>(1, std::min<int64_t>(nfull, (int64_t)occ[B] * nsm));
+  return sh;
+}
+
+static bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
 int assemble_blocks(const FeView &fe, int B) {
   int TR, cap;
   assemble_shape(B, TR, cap);
-  return (int)((fe.nnodes + TR - 1) / TR);
+  const int tiled = (int)((fe.nnodes + TR - 1) / TR);
+  return std::max(tiled, asm_bulk_shape(fe, B).grid);
 }
 
 int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B, const AsmEpilogue &epi,
@@ -1415,10 +1881,25 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
   }
   int TR, cap;
   assemble_shape(B, TR, cap);
-  const int nb = assemble_blocks(fe, B);
+  const int nb = (int)((fe.nnodes + TR - 1) / TR);   // one tile of TR nodes per CTA
   if (fe.nhang > 0) {
     hanging_sum_kernel<<<ceil_div((int64_t)fe.nhang * B, NT), NT, 0, s>>>(fe, Ycell, B);
     INVDFT_LAUNCH_CHECK();
+  }
+  // one tile per CTA by default; INVDFT_ASM_KERNEL=bulk selects the
+  // bulk-pipelined persistent variant
+  static const bool want_bulk = [] {
+    const char *v = std::getenv("INVDFT_ASM_KERNEL");
+    return v && std::string(v) == "bulk";
+  }();
+  const bool bulk_ok = want_bulk && aligned16(Ycell) && aligned16(fe.dptr) && aligned16(fe.hptr) &&
+                       aligned16(fe.inv_sqrt_mass) && (!epi.in || aligned16(epi.in)) &&
+                       (!epi.prev || aligned16(epi.prev));
+  if (bulk_ok) {
+    const AsmBulkShape sh = asm_bulk_shape(fe, B);
+    hx_assemble_bulk_kernel<<<sh.grid, NT, sh.smem, s>>>(fe, Ycell, out, B, epi, sh.TR, sh.cap);
+    INVDFT_LAUNCH_CHECK();
+    return sh.grid;
   }
   const size_t smem = sizeof(double) * (2 * (size_t)cap * B + 2 * (size_t)TR * B + TR) + sizeof(int) * 2 * (TR + 1);
   hx_assemble_tile_kernel<<<nb, NT, smem, s>>>(fe, Ycell, out, B, epi, TR, cap);

@@ -31,6 +31,7 @@ struct FeView {
   const int *hptr;          // [nnodes+1] (hanging node, weight) entries per master
   const int *hslot;         // hanging-node index of each entry
   const double *hw;
+  double *hvg;              // [ncons][B] scratch: Lowdin-gathered values of the constrained rows
   int *err;                 // device error word (bounded waits that gave up)
   const double *inv_sqrt_mass, *sqrt_mass;
 };
@@ -52,6 +53,22 @@ void launch_hx_cell_dmma(const FeView &fe, const double *H, const double *x, dou
 void launch_hx_cell_dmma_f32(const FeView &fe, const float *H32, const double *x, double *Ycell, int B,
                              int gather_mode, cudaStream_t s);
 void launch_narrow(const double *src, float *dst, int64_t n, cudaStream_t s);
+// Reference-element matrices of the matrix-free variant (passed by value, so
+// every launch carries its own copy): phi[q*n1+a] = l_a(g_q) on the GLL basis,
+// dq[q*n1+r] = derivative at g_q of the Lagrange basis on the Gauss points,
+// w = 1D Gauss weights on [0, 1].
+constexpr int kSfMaxN = 8;
+struct SfMats {
+  double phi[kSfMaxN * kSfMaxN];
+  double dq[kSfMaxN * kSfMaxN];
+  double w[kSfMaxN];
+};
+// matrix-free variant: vj [nc][nq] = v_KS * JxW at the parent quadrature points;
+// tune 0: one CTA per SM allowed the registers it wants, 1: two CTAs per SM
+void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell,
+                       int B, int gather_mode, int tune, cudaStream_t s);
+// out[i] = a[i] * b[i]
+void launch_mul(const double *a, const double *b, double *out, int64_t n, cudaStream_t s);
 // bulk-asynchronous staged variant (persistent CTAs, shared-memory panel ring)
 void launch_hx_cell_gemm_bulk(const FeView &fe, const double *H, const double *x, double *Yslot, int B,
                               int gather_mode, cudaStream_t s);

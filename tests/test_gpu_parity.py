@@ -43,6 +43,35 @@ def test_hx_matches_oracle(name, target):
         assert rel(y, orc.ops.hx(x)) < TOL_OP
 
 
+@pytest.mark.parametrize("variant", ["sf", "dmma", "rowstream"])
+@pytest.mark.parametrize("name", ["small_lih", "tiny_h2_p5"])
+def test_hx_cell_variants_match_oracle(name, variant, monkeypatch):
+    """Every cell-product variant (matrix-free sum factorisation, FP64 tensor
+    core and row-stream DFMA on stored cell matrices) gives the oracle's HX at
+    widths that exercise partial column groups and several cells per CTA."""
+    import torch
+    from invdft_b200.solver import InverseDFTSolverFunction
+    from oracle import InverseDFTSolverFunction as Oracle
+    from oracle.fe import child_to_parent_quad
+    monkeypatch.setenv("INVDFT_HX_KERNEL", variant)
+    if name == "small_lih":
+        P = problem(name)
+    else:
+        from invdft_b200.problem.system import build_problem
+        P = build_problem(name, target_solver="atoms")
+    fn = InverseDFTSolverFunction(P, native_params())
+    orc = Oracle(P, oracle_params())
+    pot = P.vxc_init.copy()
+    fn.set_potential(pot)
+    orc.ops.cell_hamiltonians(P.v_base + child_to_parent_quad(P, pot))
+    rng = np.random.default_rng(5)
+    for B in (1, 2, 5, 16, 21, 40):
+        x = rng.standard_normal((P.n_nodes, B))
+        x[~orc.free] = 0.0
+        y = fn.hx(torch.from_numpy(x).cuda()).cpu().numpy()
+        assert rel(y, orc.ops.hx(x)) < TOL_OP, (variant, B)
+
+
 @pytest.mark.parametrize("name", ["tiny_h2", "small_lih"])
 def test_eigensolve_and_density(name):
     P, fn, orc = _pair(name)

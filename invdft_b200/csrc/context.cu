@@ -319,6 +319,20 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   hptr_h.resize(hptr_h.size() + 8, hptr_h.back());
   d_dptr.upload(dptr_h, s);
   d_hptr.upload(hptr_h, s);
+  {
+    // compact numbering of the masters of hanging nodes (padded like dptr)
+    std::vector<int> midx(nn + 8, -1), mnode;
+    for (int64_t n = 0; n < nn; ++n)
+      if (hptr_h[n + 1] > hptr_h[n]) {
+        midx[n] = (int)mnode.size();
+        mnode.push_back((int)n);
+      }
+    n_masters = (int)mnode.size();
+    d_midx.upload(midx, s);
+    if (mnode.empty()) mnode.push_back(0);
+    d_mnode.upload(mnode, s);
+    d_mz.alloc((size_t)std::max(n_masters, 1) * 64);
+  }
   d_hslot.upload(hslot_h, s);
   d_zptr.upload(zptr_h, s);
   d_z.alloc((size_t)std::max(nhang, 1) * 64);
@@ -372,6 +386,7 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   fe.cons_rows = cpsi.rows.p; fe.ncons = cpsi.n;
   fe.slot_of = d_slot_of.p; fe.dptr = d_dptr.p; fe.hptr = d_hptr.p; fe.hslot = d_hslot.p; fe.hw = d_hw.p;
   fe.zptr = d_zptr.p; fe.nhang = nhang; fe.z = d_z.p;
+  fe.midx = d_midx.p; fe.mnode = d_mnode.p; fe.nmast = n_masters; fe.mz = d_mz.p;
   d_hvg.alloc((size_t)std::max(cpsi.n, 1) * 64);
   fe.hvg = d_hvg.p;
   fe.err = d_err.p;

@@ -54,6 +54,9 @@ class Context {
   int sf_tune = 0;                 // launch shape of the matrix-free kernel
   SfMats sfm{};                    // reference-element matrices of the matrix-free variant
   DevBuf<double> vj;               // [nc][nq] v_KS * JxW (matrix-free variant)
+  DevBuf<int> d_midx, d_mnode;     // compact numbering of the masters of hanging nodes
+  DevBuf<double> d_mz;             // [nmast][64] per-master hanging contributions
+  int n_masters = 0;
   DevBuf<double> d_hvg;            // [ncons][64] pre-gathered constrained rows (matrix-free variant)
   bool needs_cell_matrices() const;
   void check_device_error();

@@ -625,218 +625,16 @@ __global__ void __launch_bounds__(NT, 1) hx_gemm_bulk_kernel(FeView fe, const do
   }
 }
 
-// ---------------------------------------------------------------------------
-// HX, part 2: deterministic assembly over the node CSR + fused epilogue.
-// Thread layout (rr, j): j = column, rr = row lane; RR = NT / B rows in flight.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(NT) hx_assemble_kernel(FeView fe, const double *__restrict__ Ycell,
-                                                         double *__restrict__ out, int B,
-                                                         AsmEpilogue epi, int64_t rows_per_block) {
-  __shared__ double red[NT];
-  const int RR = NT / B;
-  const int j = threadIdx.x % B, rr = threadIdx.x / B;
-  const int64_t r0 = blockIdx.x * rows_per_block;
-  const int64_t r1 = min(fe.nnodes, r0 + rows_per_block);
-  double dot = 0.0;
-  if (rr < RR) {
-    for (int64_t n = r0 + rr; n < r1; n += RR) {
-      double acc = 0.0;
-      const int d0 = fe.dptr[n], d1 = fe.dptr[n + 1];
-      // contiguous slots of this node: independent, coalesced loads
-      for (int sl = d0; sl < d1; ++sl) acc += Ycell[(int64_t)sl * B + j];
-      for (int k = fe.hptr[n]; k < fe.hptr[n + 1]; ++k)
-        acc = fma(fe.hw[k], fe.z[(int64_t)fe.hslot[k] * B + j], acc);
-      acc *= fe.inv_sqrt_mass[n];
-      const int64_t idx = n * B + j;
-      switch (epi.kind) {
-        case AsmEpilogue::STORE: out[idx] = acc; break;
-        case AsmEpilogue::CHEB: {
-          double v = epi.alpha * (acc - epi.c * epi.in[idx]);
-          if (epi.prev) v -= epi.beta * epi.prev[idx];
-          out[idx] = v;
-          break;
-        }
-        case AsmEpilogue::VMULT: out[idx] = acc - epi.eps[j] * epi.in[idx]; break;
-        case AsmEpilogue::RHS: {
-          double v = 0.0;
-          if (d1 > d0 && fe.inv_sqrt_mass[n] != 0.0) {
-            double mu = 0.0;
-            for (int k = 0; k < B; ++k) mu = fma(epi.Mu[k * B + j], epi.psi[n * B + k], mu);
-            v = epi.occ4[j] * acc - 2.0 * fe.sqrt_mass[n] * mu;
-          }
-          out[idx] = v;
-          break;
-        }
-        case AsmEpilogue::MINRES: {
-          const double vv = epi.in[idx];
-          const double yn = acc - epi.eps[j] * vv - epi.minres_coef[j] * epi.prev[idx];
-          out[idx] = yn;
-          dot = fma(vv, yn, dot);
-          break;
-        }
-      }
-    }
-  }
-  if (epi.kind == AsmEpilogue::MINRES) {
-    red[threadIdx.x] = dot;
-    __syncthreads();
-    if (threadIdx.x < B) {
-      double s = 0.0;
-      for (int q = 0; q < RR; ++q) s += red[q * B + threadIdx.x];
-      epi.dot_partial[(int64_t)blockIdx.x * B + threadIdx.x] = s;
-    }
-  }
-}
-
-
-// ---------------------------------------------------------------------------
-// HX, part 2 (tiled): a CTA owns TR consecutive nodes, whose direct slots form
-// one contiguous segment [dptr[r0], dptr[r0+TR]).  The segment is streamed
-// into shared memory with coalesced loads and the per-node sums are taken from
-// there; hanging-node contributions (a minority) are read directly.  Thread
-// (rr, j) handles column j of nodes r0+rr, r0+rr+RR, ... (fixed order), so
-// the MINRES dot partials are deterministic.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(NT) hx_assemble_tile_kernel(FeView fe, const double *__restrict__ Ycell,
-                                                              double *__restrict__ out, int B, AsmEpilogue epi,
-                                                              int TR, int cap_slots) {
-  // shared layout: seg [cap][B] | hv [cap][B] | s_in [TR][B] | s_prev [TR][B] | ism [TR] | dp [TR+1] | hp [TR+1]
-  extern __shared__ double sm_asm[];
-  double *seg = sm_asm;
-  double *hv = seg + (size_t)cap_slots * B;
-  double *s_in = hv + (size_t)cap_slots * B;
-  double *s_prev = s_in + (size_t)TR * B;
-  double *ism = s_prev + (size_t)TR * B;
-  int *dp = reinterpret_cast<int *>(ism + TR);
-  int *hp = dp + TR + 1;
-  __shared__ double red[NT];
-  const int64_t r0 = (int64_t)blockIdx.x * TR;
-  if (r0 >= fe.nnodes) return;   // grid sized by the caller: never past the last node
-  const int rows = (int)min((int64_t)TR, fe.nnodes - r0);
-  const bool need_in = epi.kind == AsmEpilogue::CHEB || epi.kind == AsmEpilogue::VMULT ||
-                       epi.kind == AsmEpilogue::MINRES;
-  const bool need_prev = (epi.kind == AsmEpilogue::CHEB && epi.prev) || epi.kind == AsmEpilogue::MINRES;
-  // phase A: independent coalesced loads of everything the tile reads
-  stage_copy(dp, fe.dptr + r0, rows + 1);
-  stage_copy(hp, fe.hptr + r0, rows + 1);
-  stage_copy(ism, fe.inv_sqrt_mass + r0, rows);
-  if (need_in) stage_copy(s_in, epi.in + r0 * B, rows * B);
-  if (need_prev) stage_copy(s_prev, epi.prev + r0 * B, rows * B);
-  __syncthreads();
-  const int s0 = dp[0], s1 = dp[rows];
-  const bool staged = (s1 - s0) <= cap_slots;
-  if (staged) stage_copy(seg, Ycell + (int64_t)s0 * B, (s1 - s0) * B);
-  // weighted rows of the hanging nodes feeding this tile's masters, all
-  // loaded in one wave (z is small and L2-resident)
-  const int h0 = hp[0], h1 = hp[rows];
-  const bool hstaged = (h1 - h0) <= cap_slots;   // hv holds cap_slots rows of B
-  if (hstaged) {
-    constexpr int U = 8;
-    const int n = (h1 - h0) * B;
-    for (int base = threadIdx.x; base < n; base += blockDim.x * U) {
-      double v[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int i = base + u * blockDim.x;
-        const int k = h0 + i / B;
-        v[u] = i < n ? fe.hw[k] * fe.z[(int64_t)fe.hslot[k] * B + i % B] : 0.0;
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int i = base + u * blockDim.x;
-        if (i < n) hv[i] = v[u];
-      }
-    }
-  }
-  __syncthreads();
-  const int RR = NT / B;
-  const int j = threadIdx.x % B, rr = threadIdx.x / B;
-  double dot = 0.0;
-  if (rr < RR) {
-    for (int lr = rr; lr < rows; lr += RR) {
-      const int64_t n = r0 + lr;
-      const int d0 = dp[lr], d1 = dp[lr + 1];
-      double acc = 0.0;
-      if (staged) {
-        for (int sl = d0; sl < d1; ++sl) acc += seg[(sl - s0) * B + j];
-      } else {
-        for (int sl = d0; sl < d1; sl += 8) {      // eight independent loads in flight
-          double v[8];
-#pragma unroll
-          for (int u = 0; u < 8; ++u) v[u] = (sl + u < d1) ? Ycell[(int64_t)(sl + u) * B + j] : 0.0;
-#pragma unroll
-          for (int u = 0; u < 8; ++u) acc += v[u];
-        }
-      }
-      if (hstaged) {
-        for (int k = hp[lr]; k < hp[lr + 1]; ++k) acc += hv[(k - h0) * B + j];
-      } else {
-        const int k1 = hp[lr + 1];
-        for (int k = hp[lr]; k < k1; k += 8) {
-          int hs[8];
-          double w[8], v[8];
-#pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            hs[u] = (k + u < k1) ? fe.hslot[k + u] : 0;
-            w[u] = (k + u < k1) ? fe.hw[k + u] : 0.0;
-          }
-#pragma unroll
-          for (int u = 0; u < 8; ++u) v[u] = fe.z[(int64_t)hs[u] * B + j];
-#pragma unroll
-          for (int u = 0; u < 8; ++u) acc += w[u] * v[u];
-        }
-      }
-      acc *= ism[lr];
-      const int64_t idx = n * B + j;
-      const int li = lr * B + j;
-      switch (epi.kind) {
-        case AsmEpilogue::STORE: out[idx] = acc; break;
-        case AsmEpilogue::CHEB: {
-          double v = epi.alpha * (acc - epi.c * s_in[li]);
-          if (epi.prev) v -= epi.beta * s_prev[li];
-          out[idx] = v;
-          break;
-        }
-        case AsmEpilogue::VMULT: out[idx] = acc - epi.eps[j] * s_in[li]; break;
-        case AsmEpilogue::RHS: {
-          double v = 0.0;
-          if (d1 > d0 && ism[lr] != 0.0) {
-            double mu = 0.0;
-            for (int k = 0; k < B; ++k) mu = fma(epi.Mu[k * B + j], epi.psi[n * B + k], mu);
-            v = epi.occ4[j] * acc - 2.0 * fe.sqrt_mass[n] * mu;
-          }
-          out[idx] = v;
-          break;
-        }
-        case AsmEpilogue::MINRES: {
-          const double vv = s_in[li];
-          const double yn = acc - epi.eps[j] * vv - epi.minres_coef[j] * s_prev[li];
-          out[idx] = yn;
-          dot = fma(vv, yn, dot);
-          break;
-        }
-      }
-    }
-  }
-  if (epi.kind == AsmEpilogue::MINRES) {
-    red[threadIdx.x] = dot;
-    __syncthreads();
-    if (threadIdx.x < B) {
-      double sum = 0.0;
-      for (int q = 0; q < RR; ++q) sum += red[q * B + threadIdx.x];
-      epi.dot_partial[(int64_t)blockIdx.x * B + threadIdx.x] = sum;
-    }
-  }
-}
-
 // One tile of the assembly: node rows r0 .. r0+rows-1 with their direct slots
 // read from segp[sl*B + j - a0] (a shared-memory copy of the tile's slot
-// segment, or the cell results themselves with a0 = 0), their slot and
-// hanging ranges from dp/hp, M^-1/2 from ism and the epilogue inputs from
-// t_in/t_prev (tile-local, row stride B).  Thread (rr, j) handles column j of
+// segment, or the cell results themselves with a0 = 0), their slot ranges
+// from dp,
+// compact master indices from mi (-1: no hanging contributions, else the row
+// of mz), M^-1/2 from ism and the epilogue inputs from t_in/t_prev (all
+// tile-local, row stride B for blocks).  Thread (rr, j) handles column j of
 // rows rr, rr+RR, ... in a fixed order.
 __device__ __forceinline__ void assemble_tile_rows(const FeView &fe, const double *segp, int64_t a0,
-                                                   const int *dp, const int *hp, const double *ism,
+                                                   const int *dp, const int *mi, const double *ism,
                                                    const double *t_in, const double *t_prev, int64_t r0, int rows,
                                                    double *__restrict__ out, int B, const AsmEpilogue &epi,
                                                    double &dot) {
@@ -848,8 +646,8 @@ __device__ __forceinline__ void assemble_tile_rows(const FeView &fe, const doubl
     const int d0 = dp[lr], d1 = dp[lr + 1];
     double acc = 0.0;
     for (int sl = d0; sl < d1; ++sl) acc += segp[(int64_t)sl * B + j - a0];
-    const int k1 = hp[lr + 1];
-    for (int k = hp[lr]; k < k1; ++k) acc += fe.hw[k] * fe.z[(int64_t)fe.hslot[k] * B + j];
+    const int m = mi[lr];
+    if (m >= 0) acc += fe.mz[(int64_t)m * B + j];
     acc *= ism[lr];
     const int64_t idx = n * B + j;
     const int li = lr * B + j;
@@ -884,9 +682,61 @@ __device__ __forceinline__ void assemble_tile_rows(const FeView &fe, const doubl
 }
 
 // ---------------------------------------------------------------------------
+// HX, part 2 (tiled): a CTA owns TR consecutive nodes, whose direct slots form
+// one contiguous segment [dptr[r0], dptr[r0+TR]).  The segment is streamed
+// into shared memory with coalesced loads and the per-node sums are taken from
+// there; a master of hanging nodes adds its pre-summed contribution
+// mz[midx[n]] (one load).  Thread (rr, j) handles column j of nodes r0+rr,
+// r0+rr+RR, ... (fixed order), so the MINRES dot partials are deterministic.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) hx_assemble_tile_kernel(FeView fe, const double *__restrict__ Ycell,
+                                                              double *__restrict__ out, int B, AsmEpilogue epi,
+                                                              int TR, int cap_slots) {
+  // shared layout: seg [cap][B] | s_in [TR][B] | s_prev [TR][B] | ism [TR] | dp [TR+1] | mi [TR]
+  extern __shared__ double sm_asm[];
+  double *seg = sm_asm;
+  double *s_in = seg + (size_t)cap_slots * B;
+  double *s_prev = s_in + (size_t)TR * B;
+  double *ism = s_prev + (size_t)TR * B;
+  int *dp = reinterpret_cast<int *>(ism + TR);
+  int *mi = dp + TR + 1;
+  __shared__ double red[NT];
+  const int64_t r0 = (int64_t)blockIdx.x * TR;
+  if (r0 >= fe.nnodes) return;   // grid sized by the caller: never past the last node
+  const int rows = (int)min((int64_t)TR, fe.nnodes - r0);
+  const bool need_in = epi.kind == AsmEpilogue::CHEB || epi.kind == AsmEpilogue::VMULT ||
+                       epi.kind == AsmEpilogue::MINRES;
+  const bool need_prev = (epi.kind == AsmEpilogue::CHEB && epi.prev) || epi.kind == AsmEpilogue::MINRES;
+  // phase A: independent coalesced loads of everything the tile reads
+  stage_copy(dp, fe.dptr + r0, rows + 1);
+  stage_copy(mi, fe.midx + r0, rows);
+  stage_copy(ism, fe.inv_sqrt_mass + r0, rows);
+  if (need_in) stage_copy(s_in, epi.in + r0 * B, rows * B);
+  if (need_prev) stage_copy(s_prev, epi.prev + r0 * B, rows * B);
+  __syncthreads();
+  const int s0 = dp[0], s1 = dp[rows];
+  const bool staged = (s1 - s0) <= cap_slots;
+  if (staged) stage_copy(seg, Ycell + (int64_t)s0 * B, (s1 - s0) * B);
+  __syncthreads();
+  double dot = 0.0;
+  assemble_tile_rows(fe, staged ? seg : Ycell, staged ? (int64_t)s0 * B : 0, dp, mi, ism, s_in, s_prev, r0, rows,
+                     out, B, epi, dot);
+  if (epi.kind == AsmEpilogue::MINRES) {
+    const int RR = NT / B;
+    red[threadIdx.x] = dot;
+    __syncthreads();
+    if (threadIdx.x < B) {
+      double sum = 0.0;
+      for (int q = 0; q < RR; ++q) sum += red[q * B + threadIdx.x];
+      epi.dot_partial[(int64_t)blockIdx.x * B + threadIdx.x] = sum;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // HX, part 2, bulk-pipelined: persistent CTAs walk the full tiles of TR nodes
 // (tile blockIdx.x + i*gridDim.x).  Everything a tile reads is contiguous in
-// HBM -- its slot and hanging ranges, M^-1/2, the epilogue inputs and its
+// HBM -- its slot ranges, master indices, M^-1/2, the epilogue inputs and its
 // slot segment of the cell results -- so thread 0 streams tile i+1 into the
 // other of two shared-memory stages with cp.async.bulk (one mbarrier per
 // stage) while the CTA reduces tile i.  The slot segment is copied from its
@@ -898,7 +748,7 @@ __device__ __forceinline__ void assemble_tile_rows(const FeView &fe, const doubl
 // ---------------------------------------------------------------------------
 struct AsmStage {
   double *seg, *in, *prev, *ism;
-  int *dp, *hp;
+  int *dp, *mi;
 };
 
 __device__ __forceinline__ AsmStage asm_stage(unsigned char *base, int st, int TR, int cap, int B) {
@@ -911,7 +761,7 @@ __device__ __forceinline__ AsmStage asm_stage(unsigned char *base, int st, int T
   s.prev = s.in + blk;
   s.ism = s.prev + blk;
   s.dp = reinterpret_cast<int *>(s.ism + TR);
-  s.hp = s.dp + TR + 4;
+  s.mi = s.dp + TR + 4;
   return s;
 }
 
@@ -946,7 +796,7 @@ __global__ void __launch_bounds__(NT) hx_assemble_bulk_kernel(FeView fe, const d
     if (staged) bytes += 8u * (uint32_t)(a1 - a0);
     mbar_expect_tx(bar, bytes);
     bulk_g2s(S.dp, fe.dptr + r0, 4u * (TR + 4), bar);
-    bulk_g2s(S.hp, fe.hptr + r0, 4u * (TR + 4), bar);
+    bulk_g2s(S.mi, fe.midx + r0, 4u * (TR + 4), bar);
     bulk_g2s(S.ism, fe.inv_sqrt_mass + r0, 8u * TR, bar);
     if (need_in) bulk_g2s(S.in, epi.in + r0 * B, 8u * TR * B, bar);
     if (need_prev) bulk_g2s(S.prev, epi.prev + r0 * B, 8u * TR * B, bar);
@@ -989,7 +839,7 @@ __global__ void __launch_bounds__(NT) hx_assemble_bulk_kernel(FeView fe, const d
     const int s0 = S.dp[0], s1 = S.dp[TR];
     const bool staged = s1 - s0 <= cap;
     const int64_t a0 = staged ? (((int64_t)s0 * B) & ~(int64_t)1) : 0;
-    assemble_tile_rows(fe, staged ? S.seg : Ycell, a0, S.dp, S.hp, S.ism, S.in, S.prev, r0, TR, out, B, epi, dot);
+    assemble_tile_rows(fe, staged ? S.seg : Ycell, a0, S.dp, S.mi, S.ism, S.in, S.prev, r0, TR, out, B, epi, dot);
     __syncthreads();
     if (threadIdx.x == 0 && i + 2 < cnt) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1000,7 +850,7 @@ __global__ void __launch_bounds__(NT) hx_assemble_bulk_kernel(FeView fe, const d
   const int64_t rt = nfull * TR;
   if (rt < fe.nnodes && blockIdx.x == nfull % G) {
     const int rows = (int)(fe.nnodes - rt);
-    assemble_tile_rows(fe, Ycell, 0, fe.dptr + rt, fe.hptr + rt, fe.inv_sqrt_mass + rt,
+    assemble_tile_rows(fe, Ycell, 0, fe.dptr + rt, fe.midx + rt, fe.inv_sqrt_mass + rt,
                        need_in ? epi.in + rt * B : nullptr, need_prev ? epi.prev + rt * B : nullptr, rt, rows,
                        out, B, epi, dot);
   }
@@ -1024,6 +874,18 @@ __global__ void hanging_sum_kernel(FeView fe, const double *__restrict__ Ycell, 
   double acc = 0.0;
   for (int sl = fe.zptr[h]; sl < fe.zptr[h + 1]; ++sl) acc += Ycell[(int64_t)sl * B + j];
   fe.z[idx] = acc;
+}
+
+// mz[i][j] = sum_k hw[k] z[hslot[k]][j] over the (hanging node, weight)
+// entries of master mnode[i]: what C^T adds to that master, in a fixed order
+__global__ void master_sum_kernel(FeView fe, int B) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)fe.nmast * B) return;
+  const int i = (int)(idx / B), j = (int)(idx - (int64_t)i * B);
+  const int n = fe.mnode[i];
+  double acc = 0.0;
+  for (int k = fe.hptr[n]; k < fe.hptr[n + 1]; ++k) acc = fma(fe.hw[k], fe.z[(int64_t)fe.hslot[k] * B + j], acc);
+  fe.mz[idx] = acc;
 }
 
 __global__ void scale_rows_kernel(const double *d, const double *x, double *y, int64_t n, int B) {
@@ -1886,14 +1748,18 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
     hanging_sum_kernel<<<ceil_div((int64_t)fe.nhang * B, NT), NT, 0, s>>>(fe, Ycell, B);
     INVDFT_LAUNCH_CHECK();
   }
+  if (fe.nmast > 0) {
+    master_sum_kernel<<<ceil_div((int64_t)fe.nmast * B, NT), NT, 0, s>>>(fe, B);
+    INVDFT_LAUNCH_CHECK();
+  }
   // one tile per CTA by default; INVDFT_ASM_KERNEL=bulk selects the
   // bulk-pipelined persistent variant
   static const bool want_bulk = [] {
     const char *v = std::getenv("INVDFT_ASM_KERNEL");
     return v && std::string(v) == "bulk";
   }();
-  const bool bulk_ok = want_bulk && aligned16(Ycell) && aligned16(fe.dptr) && aligned16(fe.hptr) &&
-                       aligned16(fe.inv_sqrt_mass) && (!epi.in || aligned16(epi.in)) &&
+  const bool bulk_ok = want_bulk && aligned16(Ycell) && aligned16(fe.dptr) &&
+                       aligned16(fe.midx) && aligned16(fe.inv_sqrt_mass) && (!epi.in || aligned16(epi.in)) &&
                        (!epi.prev || aligned16(epi.prev));
   if (bulk_ok) {
     const AsmBulkShape sh = asm_bulk_shape(fe, B);
@@ -1901,7 +1767,7 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
     INVDFT_LAUNCH_CHECK();
     return sh.grid;
   }
-  const size_t smem = sizeof(double) * (2 * (size_t)cap * B + 2 * (size_t)TR * B + TR) + sizeof(int) * 2 * (TR + 1);
+  const size_t smem = sizeof(double) * ((size_t)cap * B + 2 * (size_t)TR * B + TR) + sizeof(int) * (2 * TR + 1);
   hx_assemble_tile_kernel<<<nb, NT, smem, s>>>(fe, Ycell, out, B, epi, TR, cap);
   INVDFT_LAUNCH_CHECK();
   return nb;

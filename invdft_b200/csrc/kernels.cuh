@@ -31,6 +31,10 @@ struct FeView {
   const int *hptr;          // [nnodes+1] (hanging node, weight) entries per master
   const int *hslot;         // hanging-node index of each entry
   const double *hw;
+  const int *midx;          // [nnodes+8] compact master index of a node (-1: no hanging contributions)
+  const int *mnode;         // [nmast] node of each master
+  int nmast;
+  double *mz;               // [nmast][B] scratch: hanging contributions summed per master
   double *hvg;              // [ncons][B] scratch: Lowdin-gathered values of the constrained rows
   int *err;                 // device error word (bounded waits that gave up)
   const double *inv_sqrt_mass, *sqrt_mass;

@@ -397,7 +397,9 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
     const std::string k = v ? v : (n1 <= kSfMaxN ? "sf" : "dmma");
     hx_variant = k == "bulk" ? 2 : (k == "rowstream" ? 1 : (k == "sf" && n1 <= kSfMaxN ? 3 : 0));
     const char *t = std::getenv("INVDFT_SF_TUNE");
-    sf_tune = t ? std::atoi(t) : (n1 <= 6 ? 1 : 0);   // two CTAs per SM where registers allow
+    // two CTAs per SM where registers allow; order 5 keeps its derivative lines
+    // in shared memory (fastest measured shape for order 5)
+    sf_tune = t ? std::atoi(t) : (n1 == 6 ? 2 : (n1 < 6 ? 1 : 0));
   }
   fe.inv_sqrt_mass = invsqrtM.p; fe.sqrt_mass = sqrtM.p;
   cv.ncc = ncc; cv.nchild_nodes = ncn; cv.cell_nodes = ch_nodes.p; cv.jxw = ch_jxw.p; cv.parent = ch_parent.p;

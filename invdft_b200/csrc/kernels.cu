@@ -372,13 +372,15 @@ __device__ __forceinline__ void sf_apply_t(const double *M, const double (&in)[N
   }
 }
 
-template <int N, int MINB>
+template <int N, int MINB, bool GXS>
 __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe, SfMats mt, const double *__restrict__ vj,
                                                                 const double *__restrict__ x,
                                                                 double *__restrict__ Ycell, int B, int C, int mode) {
+  // GXS: the weighted x-derivative lines wait in a fourth shared array instead
+  // of registers between the forward and the backward x pass
   constexpr int N2 = N * N, N3 = N2 * N;
   extern __shared__ double sm[];
-  double *A = sm, *Bs = sm + N3 * 16, *Cs = sm + 2 * N3 * 16;
+  double *A = sm, *Bs = sm + N3 * 16, *Cs = sm + 2 * N3 * 16, *Gs = sm + 3 * N3 * 16;
   const int p = threadIdx.x & 15, L = threadIdx.x >> 4;
   const int G = 16 / C;
   const int g = p / C, c = p - g * C;
@@ -427,6 +429,7 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
   sf_apply<N>(mt.dq, s, gx);
 #pragma unroll
   for (int q = 0; q < N; ++q) gx[q] *= f * mt.w[q];
+  if (GXS) sf_store<N, 0>(Gs, L, p, gx);
   __syncthreads();
   sf_load<N, 1>(A, L, p, r);             // d/dy, weighted, kept for the y back pass
   sf_apply<N>(mt.dq, r, s);
@@ -454,6 +457,7 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
   sf_store<N, 1>(A, L, p, r);
   __syncthreads();
   sf_load<N, 0>(A, L, p, r);             // x back pass, then phi^T along x
+  if (GXS) sf_load<N, 0>(Gs, L, p, gx);
   sf_apply_t<N>(mt.dq, gx, r);
 #pragma unroll
   for (int a = 0; a < N; ++a) s[a] = 0.0;
@@ -884,7 +888,22 @@ __global__ void master_sum_kernel(FeView fe, int B) {
   const int i = (int)(idx / B), j = (int)(idx - (int64_t)i * B);
   const int n = fe.mnode[i];
   double acc = 0.0;
-  for (int k = fe.hptr[n]; k < fe.hptr[n + 1]; ++k) acc = fma(fe.hw[k], fe.z[(int64_t)fe.hslot[k] * B + j], acc);
+  const int k1 = fe.hptr[n + 1];
+  constexpr int U = 16;   // sixteen loads in flight; the FMAs keep the sequential order
+  for (int k0 = fe.hptr[n]; k0 < k1; k0 += U) {
+    int hs[U];
+    double ww[U], zv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      hs[u] = k0 + u < k1 ? fe.hslot[k0 + u] : 0;
+      ww[u] = k0 + u < k1 ? fe.hw[k0 + u] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) zv[u] = k0 + u < k1 ? fe.z[(int64_t)hs[u] * B + j] : 0.0;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (k0 + u < k1) acc = fma(ww[u], zv[u], acc);
+  }
   fe.mz[idx] = acc;
 }
 
@@ -1565,19 +1584,33 @@ __global__ void hanging_gather_kernel(FeView fe, const double *__restrict__ x, i
   if (idx >= (int64_t)fe.ncons * B) return;
   const int r = (int)(idx / B), b = (int)(idx - (int64_t)r * B);
   double v = 0.0;
-  for (int t = fe.cons_ptr[r]; t < fe.cons_ptr[r + 1]; ++t)
-    v = fma(fe.cons_gw[t], x[(int64_t)fe.cons_masters[t] * B + b], v);
+  const int t1 = fe.cons_ptr[r + 1];
+  constexpr int U = 8;   // eight master loads in flight; the FMAs keep the sequential order
+  for (int t0 = fe.cons_ptr[r]; t0 < t1; t0 += U) {
+    int mm[U];
+    double ww[U], xv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      mm[u] = t0 + u < t1 ? fe.cons_masters[t0 + u] : 0;
+      ww[u] = t0 + u < t1 ? fe.cons_gw[t0 + u] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) xv[u] = t0 + u < t1 ? x[(int64_t)mm[u] * B + b] : 0.0;
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (t0 + u < t1) v = fma(ww[u], xv[u], v);
+  }
   fe.hvg[idx] = v;
 }
 
-template <int N, int MINB>
+template <int N, int MINB, bool GXS = false>
 static void hx_sf_n(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell, int B,
                     int mode, cudaStream_t s) {
   constexpr int threads = 16 * N * N;
-  const size_t smem = sizeof(double) * 3 * (size_t)N * N * N * 16;
+  const size_t smem = sizeof(double) * (GXS ? 4 : 3) * (size_t)N * N * N * 16;
   static bool attr = false;
   if (!attr) {
-    INVDFT_CUDA(cudaFuncSetAttribute(hx_cell_sf_kernel<N, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_cell_sf_kernel<N, MINB, GXS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
     attr = true;
   }
@@ -1586,7 +1619,7 @@ static void hx_sf_n(const FeView &fe, const SfMats &mt, const double *vj, const 
   while (C < B && C < 16) C <<= 1;
   const int G = 16 / C;
   const dim3 grid((unsigned)((fe.nc + G - 1) / G), (unsigned)((B + C - 1) / C));
-  hx_cell_sf_kernel<N, MINB><<<grid, threads, smem, s>>>(fe, mt, vj, x, Ycell, B, C, mode);
+  hx_cell_sf_kernel<N, MINB, GXS><<<grid, threads, smem, s>>>(fe, mt, vj, x, Ycell, B, C, mode);
   INVDFT_LAUNCH_CHECK();
 }
 
@@ -1611,7 +1644,11 @@ void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, con
     hanging_gather_kernel<<<ceil_div((int64_t)fe.ncons * B, NT), NT, 0, s>>>(fe, x, B);
     INVDFT_LAUNCH_CHECK();
   }
-  if (tune == 1 && fe.n1 <= 6) {
+  if (tune == 2 && fe.n1 == 6) {   // two CTAs per SM, derivative lines in shared memory
+    hx_sf_n<6, 2, true>(fe, mt, vj, x, Ycell, B, gather_mode, s);
+    return;
+  }
+  if (tune >= 1 && fe.n1 <= 6) {
     hx_sf_dispatch<2>(fe, mt, vj, x, Ycell, B, gather_mode, s);
     return;
   }

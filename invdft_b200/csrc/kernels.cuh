@@ -68,7 +68,8 @@ struct SfMats {
   double w[kSfMaxN];
 };
 // matrix-free variant: vj [nc][nq] = v_KS * JxW at the parent quadrature points;
-// tune 0: one CTA per SM allowed the registers it wants, 1: two CTAs per SM
+// tune 0: one CTA per SM allowed the registers it wants, 1: two CTAs per SM,
+// 2: two CTAs per SM with the derivative lines held in shared memory (order 5)
 void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell,
                        int B, int gather_mode, int tune, cudaStream_t s);
 // out[i] = a[i] * b[i]

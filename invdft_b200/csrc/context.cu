@@ -328,10 +328,25 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
         mnode.push_back((int)n);
       }
     n_masters = (int)mnode.size();
+    std::vector<int> ck0, ck1, cptr(1, 0);
+    for (int i = 0; i < n_masters; ++i) {
+      const int n = mnode[i];
+      for (int k = hptr_h[n]; k < hptr_h[n + 1]; k += kMasterChunk) {
+        ck0.push_back(k);
+        ck1.push_back(std::min(k + kMasterChunk, hptr_h[n + 1]));
+      }
+      cptr.push_back((int)ck0.size());
+    }
+    n_chunks = (int)ck0.size();
     d_midx.upload(midx, s);
     if (mnode.empty()) mnode.push_back(0);
+    if (ck0.empty()) ck0.push_back(0), ck1.push_back(0);
     d_mnode.upload(mnode, s);
+    d_ck0.upload(ck0, s);
+    d_ck1.upload(ck1, s);
+    d_cptr.upload(cptr, s);
     d_mz.alloc((size_t)std::max(n_masters, 1) * 64);
+    d_cz.alloc((size_t)std::max(n_chunks, 1) * 64);
   }
   d_hslot.upload(hslot_h, s);
   d_zptr.upload(zptr_h, s);
@@ -387,6 +402,7 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   fe.slot_of = d_slot_of.p; fe.dptr = d_dptr.p; fe.hptr = d_hptr.p; fe.hslot = d_hslot.p; fe.hw = d_hw.p;
   fe.zptr = d_zptr.p; fe.nhang = nhang; fe.z = d_z.p;
   fe.midx = d_midx.p; fe.mnode = d_mnode.p; fe.nmast = n_masters; fe.mz = d_mz.p;
+  fe.ck0 = d_ck0.p; fe.ck1 = d_ck1.p; fe.cptr = d_cptr.p; fe.nchunk = n_chunks; fe.cz = d_cz.p;
   d_hvg.alloc((size_t)std::max(cpsi.n, 1) * 64);
   fe.hvg = d_hvg.p;
   fe.err = d_err.p;

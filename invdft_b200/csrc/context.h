@@ -57,6 +57,9 @@ class Context {
   DevBuf<int> d_midx, d_mnode;     // compact numbering of the masters of hanging nodes
   DevBuf<double> d_mz;             // [nmast][64] per-master hanging contributions
   int n_masters = 0;
+  DevBuf<int> d_ck0, d_ck1, d_cptr;  // chunks of the masters' entry lists
+  DevBuf<double> d_cz;             // [nchunk][64] chunk partial sums
+  int n_chunks = 0;
   DevBuf<double> d_hvg;            // [ncons][64] pre-gathered constrained rows (matrix-free variant)
   bool needs_cell_matrices() const;
   void check_device_error();

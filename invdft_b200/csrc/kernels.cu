@@ -880,30 +880,41 @@ __global__ void hanging_sum_kernel(FeView fe, const double *__restrict__ Ycell, 
   fe.z[idx] = acc;
 }
 
-// mz[i][j] = sum_k hw[k] z[hslot[k]][j] over the (hanging node, weight)
-// entries of master mnode[i]: what C^T adds to that master, in a fixed order
-__global__ void master_sum_kernel(FeView fe, int B) {
+// What C^T adds to the masters of hanging nodes, in two balanced passes:
+// cz[c][j] = sum_k hw[k] z[hslot[k]][j] over the entries of chunk c (at most
+// kMasterChunk), then mz[i][j] = sum of the chunks of master i, both in a
+// fixed order.  (Masters carry 1 to several hundred entries; one thread per
+// master would leave the kernel waiting on the longest lists.)
+__global__ void master_chunk_kernel(FeView fe, int B) {
   const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (idx >= (int64_t)fe.nmast * B) return;
-  const int i = (int)(idx / B), j = (int)(idx - (int64_t)i * B);
-  const int n = fe.mnode[i];
+  if (idx >= (int64_t)fe.nchunk * B) return;
+  const int c = (int)(idx / B), j = (int)(idx - (int64_t)c * B);
+  const int k0 = fe.ck0[c], k1 = fe.ck1[c];
   double acc = 0.0;
-  const int k1 = fe.hptr[n + 1];
   constexpr int U = 16;   // sixteen loads in flight; the FMAs keep the sequential order
-  for (int k0 = fe.hptr[n]; k0 < k1; k0 += U) {
+  for (int kb = k0; kb < k1; kb += U) {
     int hs[U];
     double ww[U], zv[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      hs[u] = k0 + u < k1 ? fe.hslot[k0 + u] : 0;
-      ww[u] = k0 + u < k1 ? fe.hw[k0 + u] : 0.0;
+      hs[u] = kb + u < k1 ? fe.hslot[kb + u] : 0;
+      ww[u] = kb + u < k1 ? fe.hw[kb + u] : 0.0;
     }
 #pragma unroll
-    for (int u = 0; u < U; ++u) zv[u] = k0 + u < k1 ? fe.z[(int64_t)hs[u] * B + j] : 0.0;
+    for (int u = 0; u < U; ++u) zv[u] = kb + u < k1 ? fe.z[(int64_t)hs[u] * B + j] : 0.0;
 #pragma unroll
     for (int u = 0; u < U; ++u)
-      if (k0 + u < k1) acc = fma(ww[u], zv[u], acc);
+      if (kb + u < k1) acc = fma(ww[u], zv[u], acc);
   }
+  fe.cz[idx] = acc;
+}
+
+__global__ void master_sum_kernel(FeView fe, int B) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)fe.nmast * B) return;
+  const int i = (int)(idx / B), j = (int)(idx - (int64_t)i * B);
+  double acc = 0.0;
+  for (int c = fe.cptr[i]; c < fe.cptr[i + 1]; ++c) acc += fe.cz[(int64_t)c * B + j];
   fe.mz[idx] = acc;
 }
 
@@ -1722,7 +1733,7 @@ void launch_hx_cell_gemm_bulk(const FeView &fe, const double *H, const double *x
 }
 
 static void assemble_shape(int B, int &TR, int &cap) {
-  TR = std::max(8, std::min(128, 1024 / B));
+  TR = std::max(8, std::min(B <= 4 ? 512 : 128, 1024 / B));   // every thread busy at small widths
   cap = 2 * TR;   // ~1.6 slots per node on average
 }
 
@@ -1786,6 +1797,8 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
     INVDFT_LAUNCH_CHECK();
   }
   if (fe.nmast > 0) {
+    master_chunk_kernel<<<ceil_div((int64_t)fe.nchunk * B, NT), NT, 0, s>>>(fe, B);
+    INVDFT_LAUNCH_CHECK();
     master_sum_kernel<<<ceil_div((int64_t)fe.nmast * B, NT), NT, 0, s>>>(fe, B);
     INVDFT_LAUNCH_CHECK();
   }

@@ -35,10 +35,18 @@ struct FeView {
   const int *mnode;         // [nmast] node of each master
   int nmast;
   double *mz;               // [nmast][B] scratch: hanging contributions summed per master
+  // the (hanging node, weight) entries of each master split into chunks of at
+  // most kMasterChunk entries: chunk c covers entries [ck0[c], ck1[c]) and
+  // master i owns chunks [cptr[i], cptr[i+1])
+  const int *ck0, *ck1, *cptr;
+  int nchunk;
+  double *cz;               // [nchunk][B] scratch: chunk partial sums
   double *hvg;              // [ncons][B] scratch: Lowdin-gathered values of the constrained rows
   int *err;                 // device error word (bounded waits that gave up)
   const double *inv_sqrt_mass, *sqrt_mass;
 };
+
+constexpr int kMasterChunk = 32;
 
 // Gather modes of the cell GEMM.
 enum GatherMode { GATHER_LOWDIN = 0, GATHER_PLAIN = 1 };

@@ -119,13 +119,11 @@ void build_scatter(int64_t nrows, int64_t ncell, int per_cell, const int64_t *ce
 
 // Slot layout of cell results (see FeView): direct slots of free nodes sorted by
 // node then by (cell, local); rows of hanging nodes in slots after those,
-// grouped by hanging node (zptr ranges, summed into z[hanging node] first);
-// masters then receive sum_s w_sm z[s] through (hs, hw) lists sorted by
-// master, one entry per (hanging node, master) pair; Dirichlet rows dropped.
+// grouped by hanging node (zptr ranges, summed into z[hanging node] first,
+// then carried to the masters by the constraint groups); Dirichlet rows dropped.
 void build_slots(int64_t nrows, int64_t ncell, int per_cell, const int64_t *cell_nodes,
                  const invdft_constraints &c, std::vector<int> &slot_of, std::vector<int> &dptr,
-                 std::vector<int> &zptr, std::vector<int> &hptr, std::vector<int> &hs,
-                 std::vector<double> &hw) {
+                 std::vector<int> &zptr) {
   std::vector<int64_t> crow(nrows, -1), hidx(c.n_rows, -1);
   for (int64_t r = 0; r < c.n_rows; ++r) crow[c.rows[r]] = r;
   int64_t nh = 0;
@@ -133,23 +131,16 @@ void build_slots(int64_t nrows, int64_t ncell, int per_cell, const int64_t *cell
     if (c.ptr[r + 1] > c.ptr[r]) hidx[r] = nh++;
   const int64_t tot = ncell * per_cell;
   if (tot > INT32_MAX) throw StatusError(INVDFT_BAD_ARG, "more than 2^31 cell rows");
-  std::vector<int64_t> cnt(nrows + 1, 0), zcnt(nh + 1, 0), hcnt(nrows + 1, 0);
+  std::vector<int64_t> cnt(nrows + 1, 0), zcnt(nh + 1, 0);
   for (int64_t t = 0; t < tot; ++t) {
     const int64_t n = cell_nodes[t], r = crow[n];
     if (r < 0) cnt[n + 1]++;
     else if (hidx[r] >= 0) zcnt[hidx[r] + 1]++;
   }
-  for (int64_t r = 0; r < c.n_rows; ++r)
-    if (hidx[r] >= 0)
-      for (int64_t k = c.ptr[r]; k < c.ptr[r + 1]; ++k) hcnt[c.masters[k] + 1]++;
-  for (int64_t n = 0; n < nrows; ++n) {
-    cnt[n + 1] += cnt[n];
-    hcnt[n + 1] += hcnt[n];
-  }
+  for (int64_t n = 0; n < nrows; ++n) cnt[n + 1] += cnt[n];
   for (int64_t h = 0; h < nh; ++h) zcnt[h + 1] += zcnt[h];
   const int64_t ndirect = cnt[nrows];
   dptr.assign(cnt.begin(), cnt.end());
-  hptr.assign(hcnt.begin(), hcnt.end());
   zptr.resize(nh + 1);
   for (int64_t h = 0; h <= nh; ++h) zptr[h] = (int)(ndirect + zcnt[h]);
   slot_of.assign(tot, -1);
@@ -159,16 +150,73 @@ void build_slots(int64_t nrows, int64_t ncell, int per_cell, const int64_t *cell
     if (r < 0) slot_of[t] = (int)fill[n]++;
     else if (hidx[r] >= 0) slot_of[t] = (int)(ndirect + zfill[hidx[r]]++);
   }
-  hs.assign(std::max<int64_t>(hcnt[nrows], 1), 0);
-  hw.assign(std::max<int64_t>(hcnt[nrows], 1), 0.0);
-  std::vector<int64_t> hfill(hcnt.begin(), hcnt.end() - 1);
+}
+
+// Constraint rows grouped by identical ordered master lists (at most
+// kGroupRows rows per group; groups with masters first, then the Dirichlet
+// rows), the per-(group, master) partial rows, and for every master node its
+// compact index and list of partial rows, in group order.
+struct ConsGroups {
+  std::vector<int> rptr{0}, rows, hrow, m0, nm, poff, midx, mp_ptr{0}, mp_idx;
+  int ngroup = 0, ngroup_h = 0, maxnm = 0, maxnr = 0, nmast = 0, npairs = 0;
+};
+
+ConsGroups build_groups(int64_t nrows, const invdft_constraints &c) {
+  ConsGroups G;
+  std::vector<int> hidx(c.n_rows, -1);
+  int nh = 0;
   for (int64_t r = 0; r < c.n_rows; ++r)
-    if (hidx[r] >= 0)
-      for (int64_t k = c.ptr[r]; k < c.ptr[r + 1]; ++k) {
-        const int64_t m = c.masters[k];
-        hs[hfill[m]] = (int)hidx[r];
-        hw[hfill[m]++] = c.weights[k];
-      }
+    if (c.ptr[r + 1] > c.ptr[r]) hidx[r] = nh++;
+  std::map<std::vector<int64_t>, int> key;
+  std::vector<std::vector<int>> members;
+  for (int64_t r = 0; r < c.n_rows; ++r) {
+    if (hidx[r] < 0) continue;
+    std::vector<int64_t> k(c.masters + c.ptr[r], c.masters + c.ptr[r + 1]);
+    auto it = key.find(k);
+    if (it == key.end()) {
+      it = key.emplace(std::move(k), (int)members.size()).first;
+      members.emplace_back();
+    }
+    members[it->second].push_back((int)r);
+  }
+  auto emit = [&](const std::vector<int> &L, size_t a, size_t b, int m0, int nm) {
+    for (size_t q = a; q < b; ++q) {
+      G.rows.push_back(L[q]);
+      G.hrow.push_back(hidx[L[q]]);
+    }
+    G.rptr.push_back((int)G.rows.size());
+    G.m0.push_back(m0);
+    G.nm.push_back(nm);
+    G.poff.push_back(G.npairs);
+    G.npairs += nm;
+    G.maxnm = std::max(G.maxnm, nm);
+    G.maxnr = std::max(G.maxnr, (int)(b - a));
+  };
+  for (const auto &L : members) {
+    const int m0 = (int)c.ptr[L[0]], nm = (int)(c.ptr[L[0] + 1] - c.ptr[L[0]]);
+    for (size_t a = 0; a < L.size(); a += kGroupRows) emit(L, a, std::min(L.size(), a + kGroupRows), m0, nm);
+  }
+  G.ngroup_h = (int)G.nm.size();
+  std::vector<int> dir;
+  for (int64_t r = 0; r < c.n_rows; ++r)
+    if (hidx[r] < 0) dir.push_back((int)r);
+  for (size_t a = 0; a < dir.size(); a += kGroupRows) emit(dir, a, std::min(dir.size(), a + kGroupRows), 0, 0);
+  G.ngroup = (int)G.nm.size();
+  // masters: compact numbering in node order, partial rows in group order
+  std::vector<int> cnt(nrows, 0);
+  for (int g = 0; g < G.ngroup_h; ++g)
+    for (int t = 0; t < G.nm[g]; ++t) cnt[c.masters[G.m0[g] + t]]++;
+  G.midx.assign(nrows + 8, -1);
+  for (int64_t n = 0; n < nrows; ++n)
+    if (cnt[n] > 0) {
+      G.midx[n] = G.nmast++;
+      G.mp_ptr.push_back(G.mp_ptr.back() + cnt[n]);
+    }
+  std::vector<int> fill(G.mp_ptr.begin(), G.mp_ptr.end() - 1);
+  G.mp_idx.assign(std::max(G.mp_ptr.back(), 1), 0);
+  for (int g = 0; g < G.ngroup_h; ++g)
+    for (int t = 0; t < G.nm[g]; ++t) G.mp_idx[fill[G.midx[c.masters[G.m0[g] + t]]]++] = G.poff[g] + t;
+  return G;
 }
 
 }  // namespace
@@ -292,9 +340,8 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   const int64_t nmast = d->cons_psi.n_rows ? d->cons_psi.ptr[d->cons_psi.n_rows] : 0;
   std::vector<double> cgw(std::max<int64_t>(nmast, 1), 0.0);
   for (int64_t k = 0; k < nmast; ++k) cgw[k] = d->cons_psi.weights[k] * ism[d->cons_psi.masters[k]];
-  std::vector<int> slot_of, dptr_h, zptr_h, hptr_h, hslot_h;
-  std::vector<double> hw_h;
-  build_slots(nn, nc, nd, d->cell_nodes, d->cons_psi, slot_of, dptr_h, zptr_h, hptr_h, hslot_h, hw_h);
+  std::vector<int> slot_of, dptr_h, zptr_h;
+  build_slots(nn, nc, nd, d->cell_nodes, d->cons_psi, slot_of, dptr_h, zptr_h);
   nhang = (int)zptr_h.size() - 1;
 
   phi.upload(ph, s);
@@ -316,42 +363,26 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   // eight entries of padding: the pipelined assembly copies slot ranges in
   // 16-byte units and may read up to three entries past the last node
   dptr_h.resize(dptr_h.size() + 8, dptr_h.back());
-  hptr_h.resize(hptr_h.size() + 8, hptr_h.back());
   d_dptr.upload(dptr_h, s);
-  d_hptr.upload(hptr_h, s);
   {
-    // compact numbering of the masters of hanging nodes (padded like dptr)
-    std::vector<int> midx(nn + 8, -1), mnode;
-    for (int64_t n = 0; n < nn; ++n)
-      if (hptr_h[n + 1] > hptr_h[n]) {
-        midx[n] = (int)mnode.size();
-        mnode.push_back((int)n);
-      }
-    n_masters = (int)mnode.size();
-    std::vector<int> ck0, ck1, cptr(1, 0);
-    for (int i = 0; i < n_masters; ++i) {
-      const int n = mnode[i];
-      for (int k = hptr_h[n]; k < hptr_h[n + 1]; k += kMasterChunk) {
-        ck0.push_back(k);
-        ck1.push_back(std::min(k + kMasterChunk, hptr_h[n + 1]));
-      }
-      cptr.push_back((int)ck0.size());
-    }
-    n_chunks = (int)ck0.size();
-    d_midx.upload(midx, s);
-    if (mnode.empty()) mnode.push_back(0);
-    if (ck0.empty()) ck0.push_back(0), ck1.push_back(0);
-    d_mnode.upload(mnode, s);
-    d_ck0.upload(ck0, s);
-    d_ck1.upload(ck1, s);
-    d_cptr.upload(cptr, s);
-    d_mz.alloc((size_t)std::max(n_masters, 1) * 64);
-    d_cz.alloc((size_t)std::max(n_chunks, 1) * 64);
+    const ConsGroups G = build_groups(nn, d->cons_psi);
+    n_masters = G.nmast;
+    d_midx.upload(G.midx, s);
+    d_g_rptr.upload(G.rptr, s);
+    d_g_rows.upload(G.rows.empty() ? std::vector<int>{0} : G.rows, s);
+    d_g_hrow.upload(G.hrow.empty() ? std::vector<int>{0} : G.hrow, s);
+    d_g_m0.upload(G.m0.empty() ? std::vector<int>{0} : G.m0, s);
+    d_g_nm.upload(G.nm.empty() ? std::vector<int>{0} : G.nm, s);
+    d_g_poff.upload(G.poff.empty() ? std::vector<int>{0} : G.poff, s);
+    d_mp_ptr.upload(G.mp_ptr, s);
+    d_mp_idx.upload(G.mp_idx, s);
+    d_mz.alloc((size_t)std::max(G.nmast, 1) * 64);
+    d_gpart.alloc((size_t)std::max(G.npairs, 1) * 64);
+    fe.ngroup = G.ngroup; fe.ngroup_h = G.ngroup_h; fe.g_maxnm = G.maxnm; fe.g_maxnr = G.maxnr;
+    check((size_t)std::max(G.maxnm, 1) * (64 + kGroupRows) * 8 <= 200 * 1024, "a constraint row has too many masters");
   }
-  d_hslot.upload(hslot_h, s);
   d_zptr.upload(zptr_h, s);
   d_z.alloc((size_t)std::max(nhang, 1) * 64);
-  d_hw.upload(hw_h, s);
   d_err.alloc(1);
   d_err.zero(s);
   sqrtM.upload(sm, s);
@@ -399,10 +430,12 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   fe.phi = phi.p; fe.cell_h = cell_h.p; fe.cell_nodes = cell_nodes.p; fe.cell_map = cell_map.p;
   fe.cons_ptr = cpsi.ptr.p; fe.cons_masters = cpsi.masters.p; fe.cons_w = cpsi.w.p; fe.cons_gw = cons_gw.p;
   fe.cons_rows = cpsi.rows.p; fe.ncons = cpsi.n;
-  fe.slot_of = d_slot_of.p; fe.dptr = d_dptr.p; fe.hptr = d_hptr.p; fe.hslot = d_hslot.p; fe.hw = d_hw.p;
+  fe.slot_of = d_slot_of.p; fe.dptr = d_dptr.p;
   fe.zptr = d_zptr.p; fe.nhang = nhang; fe.z = d_z.p;
-  fe.midx = d_midx.p; fe.mnode = d_mnode.p; fe.nmast = n_masters; fe.mz = d_mz.p;
-  fe.ck0 = d_ck0.p; fe.ck1 = d_ck1.p; fe.cptr = d_cptr.p; fe.nchunk = n_chunks; fe.cz = d_cz.p;
+  fe.midx = d_midx.p; fe.nmast = n_masters; fe.mz = d_mz.p;
+  fe.g_rptr = d_g_rptr.p; fe.g_rows = d_g_rows.p; fe.g_hrow = d_g_hrow.p; fe.g_m0 = d_g_m0.p;
+  fe.g_nm = d_g_nm.p; fe.g_poff = d_g_poff.p; fe.mp_ptr = d_mp_ptr.p; fe.mp_idx = d_mp_idx.p;
+  fe.gpart = d_gpart.p;
   d_hvg.alloc((size_t)std::max(cpsi.n, 1) * 64);
   fe.hvg = d_hvg.p;
   fe.err = d_err.p;

@@ -43,10 +43,9 @@ class Context {
   DevBuf<int> cell_nodes, cell_map;
   Cons cpsi, cadj, cchild;
   DevBuf<double> cons_gw;
-  DevBuf<int> d_slot_of, d_dptr, d_hptr, d_hslot, d_err, d_zptr;
+  DevBuf<int> d_slot_of, d_dptr, d_err, d_zptr;
   DevBuf<double> d_z;
   int nhang = 0;
-  DevBuf<double> d_hw;
   int ldh = 0;
   // cell products: 3 matrix-free sum factorisation (default), 0 FP64 tensor core
   // on stored cell matrices (mma.sync f64), 1 row-stream DFMA, 2 bulk-staged DFMA
@@ -54,12 +53,12 @@ class Context {
   int sf_tune = 0;                 // launch shape of the matrix-free kernel
   SfMats sfm{};                    // reference-element matrices of the matrix-free variant
   DevBuf<double> vj;               // [nc][nq] v_KS * JxW (matrix-free variant)
-  DevBuf<int> d_midx, d_mnode;     // compact numbering of the masters of hanging nodes
+  DevBuf<int> d_midx;              // compact numbering of the masters of hanging nodes
   DevBuf<double> d_mz;             // [nmast][64] per-master hanging contributions
   int n_masters = 0;
-  DevBuf<int> d_ck0, d_ck1, d_cptr;  // chunks of the masters' entry lists
-  DevBuf<double> d_cz;             // [nchunk][64] chunk partial sums
-  int n_chunks = 0;
+  // constraint groups (rows with identical master lists) and master pair lists
+  DevBuf<int> d_g_rptr, d_g_rows, d_g_hrow, d_g_m0, d_g_nm, d_g_poff, d_mp_ptr, d_mp_idx;
+  DevBuf<double> d_gpart;          // [npairs][64] per-(group, master) partial sums
   DevBuf<double> d_hvg;            // [ncons][64] pre-gathered constrained rows (matrix-free variant)
   bool needs_cell_matrices() const;
   void check_device_error();

@@ -880,33 +880,33 @@ __global__ void hanging_sum_kernel(FeView fe, const double *__restrict__ Ycell, 
   fe.z[idx] = acc;
 }
 
-// What C^T adds to the masters of hanging nodes, in two balanced passes:
-// cz[c][j] = sum_k hw[k] z[hslot[k]][j] over the entries of chunk c (at most
-// kMasterChunk), then mz[i][j] = sum of the chunks of master i, both in a
-// fixed order.  (Masters carry 1 to several hundred entries; one thread per
-// master would leave the kernel waiting on the longest lists.)
-__global__ void master_chunk_kernel(FeView fe, int B) {
-  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (idx >= (int64_t)fe.nchunk * B) return;
-  const int c = (int)(idx / B), j = (int)(idx - (int64_t)c * B);
-  const int k0 = fe.ck0[c], k1 = fe.ck1[c];
-  double acc = 0.0;
-  constexpr int U = 16;   // sixteen loads in flight; the FMAs keep the sequential order
-  for (int kb = k0; kb < k1; kb += U) {
-    int hs[U];
-    double ww[U], zv[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      hs[u] = kb + u < k1 ? fe.hslot[kb + u] : 0;
-      ww[u] = kb + u < k1 ? fe.hw[kb + u] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) zv[u] = kb + u < k1 ? fe.z[(int64_t)hs[u] * B + j] : 0.0;
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-      if (kb + u < k1) acc = fma(ww[u], zv[u], acc);
+// What C^T adds to the masters of hanging nodes, in two passes.  One CTA per
+// hanging constraint group reads the group's z rows and weights once into
+// shared memory
+// and writes gpart[g_poff[g] + t][j] = sum_q w[row q, t] z[row q][j] for each
+// of its masters t; then mz[i][j] sums master i's (group, master) partials,
+// both in a fixed order.
+__global__ void __launch_bounds__(NT) group_partial_kernel(FeView fe, int B) {
+  extern __shared__ double sp[];   // zr [nr][B] | wm [nr][nm]
+  const int g = blockIdx.x;
+  const int nm = fe.g_nm[g], rp0 = fe.g_rptr[g], nr = fe.g_rptr[g + 1] - rp0;
+  double *zr = sp, *wm = sp + (size_t)nr * B;
+  for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
+    const int q = i / B, j = i - q * B;
+    zr[i] = fe.z[(int64_t)fe.g_hrow[rp0 + q] * B + j];
   }
-  fe.cz[idx] = acc;
+  for (int i = threadIdx.x; i < nr * nm; i += blockDim.x) {
+    const int q = i / nm, t = i - q * nm;
+    wm[i] = fe.cons_w[fe.cons_ptr[fe.g_rows[rp0 + q]] + t];
+  }
+  __syncthreads();
+  const int64_t po = fe.g_poff[g];
+  for (int i = threadIdx.x; i < nm * B; i += blockDim.x) {
+    const int t = i / B, j = i - t * B;
+    double acc = 0.0;
+    for (int q = 0; q < nr; ++q) acc = fma(wm[q * nm + t], zr[q * B + j], acc);
+    fe.gpart[(po + t) * B + j] = acc;
+  }
 }
 
 __global__ void master_sum_kernel(FeView fe, int B) {
@@ -914,7 +914,7 @@ __global__ void master_sum_kernel(FeView fe, int B) {
   if (idx >= (int64_t)fe.nmast * B) return;
   const int i = (int)(idx / B), j = (int)(idx - (int64_t)i * B);
   double acc = 0.0;
-  for (int c = fe.cptr[i]; c < fe.cptr[i + 1]; ++c) acc += fe.cz[(int64_t)c * B + j];
+  for (int q = fe.mp_ptr[i]; q < fe.mp_ptr[i + 1]; ++q) acc += fe.gpart[(int64_t)fe.mp_idx[q] * B + j];
   fe.mz[idx] = acc;
 }
 
@@ -1588,30 +1588,31 @@ void launch_hx_cell_dmma_f32(const FeView &fe, const float *H32, const double *x
 }
 
 // hvg[r][b] = sum_t gw_t x[master_t][b] for every constrained row r: the
-// Lowdin gather of the hanging (and Dirichlet) rows, in the same FMA order as
-// gather_value, so the matrix-free kernel reads them with one load each
-__global__ void hanging_gather_kernel(FeView fe, const double *__restrict__ x, int B) {
-  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (idx >= (int64_t)fe.ncons * B) return;
-  const int r = (int)(idx / B), b = (int)(idx - (int64_t)r * B);
-  double v = 0.0;
-  const int t1 = fe.cons_ptr[r + 1];
-  constexpr int U = 8;   // eight master loads in flight; the FMAs keep the sequential order
-  for (int t0 = fe.cons_ptr[r]; t0 < t1; t0 += U) {
-    int mm[U];
-    double ww[U], xv[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      mm[u] = t0 + u < t1 ? fe.cons_masters[t0 + u] : 0;
-      ww[u] = t0 + u < t1 ? fe.cons_gw[t0 + u] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u) xv[u] = t0 + u < t1 ? x[(int64_t)mm[u] * B + b] : 0.0;
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-      if (t0 + u < t1) v = fma(ww[u], xv[u], v);
+// Lowdin gather of the hanging (and, as zeros, the Dirichlet) rows, in the
+// FMA order of gather_value, so the matrix-free kernel reads each with one
+// load.  One CTA per constraint group: the group's master rows and weights
+// are read once into shared memory and serve all of its rows.
+__global__ void __launch_bounds__(NT) group_gather_kernel(FeView fe, const double *__restrict__ x, int B) {
+  extern __shared__ double sg[];   // xm [nm][B] | wm [nr][nm]
+  const int g = blockIdx.x;
+  const int nm = fe.g_nm[g], m0 = fe.g_m0[g];
+  const int rp0 = fe.g_rptr[g], nr = fe.g_rptr[g + 1] - rp0;
+  double *xm = sg, *wm = sg + (size_t)nm * B;
+  for (int i = threadIdx.x; i < nm * B; i += blockDim.x) {
+    const int t = i / B, j = i - t * B;
+    xm[i] = x[(int64_t)fe.cons_masters[m0 + t] * B + j];
   }
-  fe.hvg[idx] = v;
+  for (int i = threadIdx.x; i < nr * nm; i += blockDim.x) {
+    const int q = i / nm, t = i - q * nm;
+    wm[i] = fe.cons_gw[fe.cons_ptr[fe.g_rows[rp0 + q]] + t];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
+    const int q = i / B, j = i - q * B;
+    double v = 0.0;
+    for (int t = 0; t < nm; ++t) v = fma(wm[q * nm + t], xm[t * B + j], v);
+    fe.hvg[(int64_t)fe.g_rows[rp0 + q] * B + j] = v;
+  }
 }
 
 template <int N, int MINB, bool GXS = false>
@@ -1651,8 +1652,14 @@ static void hx_sf_dispatch(const FeView &fe, const SfMats &mt, const double *vj,
 
 void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell,
                        int B, int gather_mode, int tune, cudaStream_t s) {
-  if (gather_mode != GATHER_PLAIN && fe.ncons > 0) {
-    hanging_gather_kernel<<<ceil_div((int64_t)fe.ncons * B, NT), NT, 0, s>>>(fe, x, B);
+  if (gather_mode != GATHER_PLAIN && fe.ngroup > 0) {
+    const size_t smem = sizeof(double) * (size_t)std::max(fe.g_maxnm, 1) * (B + fe.g_maxnr);
+    static bool attr = false;
+    if (!attr) {
+      INVDFT_CUDA(cudaFuncSetAttribute(group_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+      attr = true;
+    }
+    group_gather_kernel<<<fe.ngroup, NT, smem, s>>>(fe, x, B);
     INVDFT_LAUNCH_CHECK();
   }
   if (tune == 2 && fe.n1 == 6) {   // two CTAs per SM, derivative lines in shared memory
@@ -1797,7 +1804,13 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
     INVDFT_LAUNCH_CHECK();
   }
   if (fe.nmast > 0) {
-    master_chunk_kernel<<<ceil_div((int64_t)fe.nchunk * B, NT), NT, 0, s>>>(fe, B);
+    const size_t smem = sizeof(double) * (size_t)std::max(fe.g_maxnr, 1) * (B + std::max(fe.g_maxnm, 1));
+    static bool attr = false;
+    if (!attr) {
+      INVDFT_CUDA(cudaFuncSetAttribute(group_partial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+      attr = true;
+    }
+    group_partial_kernel<<<fe.ngroup_h, NT, smem, s>>>(fe, B);
     INVDFT_LAUNCH_CHECK();
     master_sum_kernel<<<ceil_div((int64_t)fe.nmast * B, NT), NT, 0, s>>>(fe, B);
     INVDFT_LAUNCH_CHECK();

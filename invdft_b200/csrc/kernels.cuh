@@ -22,31 +22,32 @@ struct FeView {
   // slot layout of cell results: row (cell, local) of a cell product is written
   // to slot slot_of[cell*nd+local] (-1: Dirichlet row, dropped).  Free nodes own
   // the contiguous slots [dptr[n], dptr[n+1]); rows of hanging nodes live in
-  // slots after those and reach their masters through (hslot, hw) lists.
+  // slots after those, are summed per hanging node into z and reach their
+  // masters through the constraint groups below.
   const int *slot_of;       // [nc*nd]
   const int *dptr;          // [nnodes+1]
   const int *zptr;          // [nhang+1] slot ranges of the hanging nodes' rows
   int nhang;
   double *z;                // [nhang][B] scratch: summed rows of each hanging node
-  const int *hptr;          // [nnodes+1] (hanging node, weight) entries per master
-  const int *hslot;         // hanging-node index of each entry
-  const double *hw;
   const int *midx;          // [nnodes+8] compact master index of a node (-1: no hanging contributions)
-  const int *mnode;         // [nmast] node of each master
   int nmast;
   double *mz;               // [nmast][B] scratch: hanging contributions summed per master
-  // the (hanging node, weight) entries of each master split into chunks of at
-  // most kMasterChunk entries: chunk c covers entries [ck0[c], ck1[c]) and
-  // master i owns chunks [cptr[i], cptr[i+1])
-  const int *ck0, *ck1, *cptr;
-  int nchunk;
-  double *cz;               // [nchunk][B] scratch: chunk partial sums
+  // constraint rows grouped by identical (ordered) master lists: group g owns
+  // rows g_rows[g_rptr[g] .. g_rptr[g+1]) (hanging indices g_hrow, -1 for
+  // Dirichlet rows), whose masters are cons_masters[g_m0[g] ..][0, g_nm[g]);
+  // groups [0, ngroup_h) have masters, the rest are Dirichlet rows.  Pair
+  // (g, t) of a hanging group is partial row g_poff[g] + t; master i sums the
+  // partial rows mp_idx[mp_ptr[i] .. mp_ptr[i+1]).
+  int ngroup, ngroup_h, g_maxnm, g_maxnr;
+  const int *g_rptr, *g_rows, *g_hrow, *g_m0, *g_nm, *g_poff;
+  const int *mp_ptr, *mp_idx;
+  double *gpart;            // [npairs][B] scratch: per (group, master) partial sums
   double *hvg;              // [ncons][B] scratch: Lowdin-gathered values of the constrained rows
   int *err;                 // device error word (bounded waits that gave up)
   const double *inv_sqrt_mass, *sqrt_mass;
 };
 
-constexpr int kMasterChunk = 32;
+constexpr int kGroupRows = 64;   // constraint rows per group at most
 
 // Gather modes of the cell GEMM.
 enum GatherMode { GATHER_LOWDIN = 0, GATHER_PLAIN = 1 };

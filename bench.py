@@ -143,6 +143,29 @@ def build_workload(name: str, rank: int):
     return P, dict(t_mesh_s=round(t_mesh, 1), t_setup_s=round(time.time() - t0, 1))
 
 
+def hx_probe(args, dev):
+    """``--steps`` Lowdin HX applications of a seeded [n_nodes, width] block on
+    the workload's mesh at v_xc = the initial guess: the launch sequence the
+    kernel profiles in profiles/ are captured on."""
+    import torch
+    from invdft_b200.problem.system import build_problem
+    from invdft_b200.solver import InverseDFTSolverFunction
+    P = build_problem(args.config, target_solver="atoms")
+    fn = InverseDFTSolverFunction(P, force_params("fp64"))
+    fn.set_potential(P.vxc_init.copy())
+    g = torch.Generator(device=dev).manual_seed(1)
+    x = torch.randn(P.n_nodes, args.hx_width, dtype=torch.float64, device=dev, generator=g)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        y = fn.hx(x)
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"probe": "hx", "workload": args.config, "width": args.hx_width, "applications": args.steps,
+                      "ms_per_hx": e0.elapsed_time(e1) / max(args.steps, 1), "norm": float(y.norm())}))
+    fn.close()
+
+
 def aggregate(ms: float, e2e_s: float, steps: int, world: int, dist=None, device="cuda"):
     """Whole-job throughput of ``world`` replicas timed as the max over ranks.
 
@@ -202,6 +225,9 @@ def main():
                     help="do not time the FP64 path on the same trajectory")
     ap.add_argument("--cpu-sample-cells", type=int, default=400)
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample (profiling runs)")
+    ap.add_argument("--hx-width", type=int, default=0,
+                    help="kernel probe for profiling: --steps Lowdin HX applications of a seeded block of this "
+                         "width at v_xc = the initial guess, timed with CUDA events (no force evaluation)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -217,6 +243,10 @@ def main():
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     threads = os.cpu_count() or 1
+
+    if args.hx_width > 0:
+        hx_probe(args, dev)
+        return
 
     if args.impl == "reference":
         if rank != 0:
@@ -283,8 +313,11 @@ def main():
     peaks, pk = _peaks()
     matrix_free = os.environ.get("INVDFT_HX_KERNEL", "sf") == "sf" and P.p <= 7 and args.precision == "fp64"
     hbm_achieved = gemm_bytes / (gemm_ms / 1000.0) / 1e9 if gemm_ms > 0 else None
-    per_launch_traffic = _traffic_from_profiles(
-        f"{args.config}:{'sf' if matrix_free else 'dmma'}:{args.precision}")
+    # captured traffic of one launch of a given width, scaled to the mean width
+    # of this run's launches (traffic grows with the columns processed)
+    cap = _traffic_from_profiles(f"{args.config}:{'sf' if matrix_free else 'dmma'}:{args.precision}")
+    mean_cols = sum(s["n_hx_columns"] for s in stats) / max(n_gemm, 1)
+    per_launch_traffic = cap["bytes"] * mean_cols / cap["columns"] if isinstance(cap, dict) else cap
     if matrix_free:
         fp64_peak = _fp64_peak_tflops(dev)
         achieved = gemm_flops / (gemm_ms / 1000.0) / 1e12 if gemm_ms > 0 else None

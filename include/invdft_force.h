@@ -200,6 +200,22 @@ invdft_status invdft_force_backward(invdft_ctx *ctx, double *force, invdft_force
  * Hamiltonians (setVEff + computeCellHamiltonianMatrix, :1367-1388). */
 invdft_status invdft_set_potential(invdft_ctx *ctx, const double *pot);
 
+/* POST_PROCESS projection of v_xc to the parent mesh (InverseDFTEngine::
+ * projectVxcToParentMesh, InverseDFTEngine.cpp:3462-3545, called from
+ * interpolateVxc :3241-3248): vxc_child [n_child_nodes] (child constraints are
+ * distributed first), parent_nodal [n_nodes] = lumped-mass L2 projection of
+ * v_xc + factorForLDAVxc * v_LDA at the parent quadrature points, with the psi
+ * constraints distributed.  Host arrays; pot and force state are untouched. */
+invdft_status invdft_project_vxc_to_parent(invdft_ctx *ctx, const double *vxc_child, double *parent_nodal);
+
+/* A parent nodal field at points (the writeToPoints branch of
+ * InverseDFTEngine::interpolateVxc, InverseDFTEngine.cpp:3275-3456): point i
+ * lies in parent cell cells[i] at reference coordinates xi[3i..3i+2] in
+ * [0, 1]^3 (x, y, z); out[i] = sum_l parent_nodal[node(cell, l)] N_l(xi).
+ * Host arrays. */
+invdft_status invdft_evaluate_parent_field(invdft_ctx *ctx, const double *parent_nodal, int64_t npts,
+                                           const int64_t *cells, const double *xi, double *out);
+
 /* Lowdin HX on device blocks: d_y = M^-1/2 C^T sum_e H_e (C M^-1/2 d_x)_e
  * (KohnShamDFTBaseOperator::HXWithLowdinOrthonormalisedInput as called at
  * MultiVectorAdjointLinearSolverProblem.cpp:1353).  B in [1, 64]. */

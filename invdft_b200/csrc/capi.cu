@@ -192,6 +192,22 @@ invdft_status invdft_set_potential(invdft_ctx *ctx, const double *pot) {
   });
 }
 
+invdft_status invdft_project_vxc_to_parent(invdft_ctx *ctx, const double *vxc_child, double *parent_nodal) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!vxc_child || !parent_nodal) throw invdft::StatusError(INVDFT_BAD_ARG, "null array");
+    c.project_vxc_to_parent(vxc_child, parent_nodal);
+  });
+}
+
+invdft_status invdft_evaluate_parent_field(invdft_ctx *ctx, const double *parent_nodal, int64_t npts,
+                                           const int64_t *cells, const double *xi, double *out) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!parent_nodal || npts < 0 || (npts > 0 && (!cells || !xi || !out)))
+      throw invdft::StatusError(INVDFT_BAD_ARG, "null array or negative point count");
+    c.evaluate_parent_field(parent_nodal, npts, cells, xi, out);
+  });
+}
+
 invdft_status invdft_hx(invdft_ctx *ctx, const double *d_x, double *d_y, int32_t B) {
   return guard(ctx, [&](invdft::Context &c) {
     if (!d_x || !d_y || B < 1 || B > 64) throw invdft::StatusError(INVDFT_BAD_ARG, "bad hx arguments (B in [1, 64])");

@@ -445,10 +445,11 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
     const char *v = std::getenv("INVDFT_HX_KERNEL");
     const std::string k = v ? v : (n1 <= kSfMaxN ? "sf" : "dmma");
     hx_variant = k == "bulk" ? 2 : (k == "rowstream" ? 1 : (k == "sf" && n1 <= kSfMaxN ? 3 : 0));
+    // INVDFT_SF_TUNE pins the launch shape; otherwise each block width is
+    // autotuned on its first use (sf_shape)
     const char *t = std::getenv("INVDFT_SF_TUNE");
-    // two CTAs per SM where registers allow; order 5 keeps its derivative lines
-    // in shared memory (fastest measured shape for order 5)
-    sf_tune = t ? std::atoi(t) : (n1 == 6 ? 2 : (n1 < 6 ? 1 : 0));
+    sf_tune = t ? std::atoi(t) : -1;
+    for (int &v : sf_tuned) v = -1;
   }
   fe.inv_sqrt_mass = invsqrtM.p; fe.sqrt_mass = sqrtM.p;
   cv.ncc = ncc; cv.nchild_nodes = ncn; cv.cell_nodes = ch_nodes.p; cv.jxw = ch_jxw.p; cv.parent = ch_parent.p;
@@ -535,11 +536,48 @@ void Context::set_subspace(const double *Xh) {
 // ---------------------------------------------------------------------------
 // Hamiltonian application and the eigensolver
 // ---------------------------------------------------------------------------
+// Launch shape of the matrix-free cell product for width Bw: pinned by
+// INVDFT_SF_TUNE, else measured once per width among the shapes compiled for
+// this order (one warm-up and two timed launches each, on the real block) and
+// the fastest kept.  Every shape runs the same FMA sequence, so the choice
+// changes timing only, never results.
+int Context::sf_shape(const double *d_x, int Bw) {
+  if (sf_tune >= 0) return sf_tune;
+  int &t = sf_tuned[std::min(std::max(Bw, 0), 64)];
+  if (t >= 0) return t;
+  std::vector<int> cand = {0};
+  if (n1 <= 6) cand.push_back(1);
+  if (n1 == 6) cand.push_back(2);
+  if (cand.size() == 1) return t = 0;
+  cudaEvent_t a, b;
+  INVDFT_CUDA(cudaEventCreate(&a));
+  INVDFT_CUDA(cudaEventCreate(&b));
+  float best = 0.f;
+  int arg = cand.back();
+  for (size_t k = 0; k < cand.size(); ++k) {
+    launch_hx_cell_sf(fe, sfm, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, cand[k], stream);
+    INVDFT_CUDA(cudaEventRecord(a, stream));
+    for (int r = 0; r < 2; ++r) launch_hx_cell_sf(fe, sfm, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, cand[k], stream);
+    INVDFT_CUDA(cudaEventRecord(b, stream));
+    INVDFT_CUDA(cudaEventSynchronize(b));
+    float ms = 0.f;
+    INVDFT_CUDA(cudaEventElapsedTime(&ms, a, b));
+    if (k == 0 || ms < best) {
+      best = ms;
+      arg = cand[k];
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return t = arg;
+}
+
 void Context::cell_gemm(const double *d_x, int Bw, bool low) {
+  const int shape = (!low && hx_variant == 3) ? sf_shape(d_x, Bw) : 0;   // tuning stays outside the timing
   const bool rec = profile && ev_used + 2 <= (int)ev_pool.size();
   if (rec) INVDFT_CUDA(cudaEventRecord(ev_pool[ev_used], stream));
   if (low) launch_hx_cell_dmma_f32(fe, H32.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
-  else if (hx_variant == 3) launch_hx_cell_sf(fe, sfm, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, sf_tune, stream);
+  else if (hx_variant == 3) launch_hx_cell_sf(fe, sfm, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, shape, stream);
   else if (hx_variant == 0) launch_hx_cell_dmma(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
   else if (hx_variant == 2) launch_hx_cell_gemm_bulk(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
   else launch_hx_cell_gemm(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
@@ -592,6 +630,49 @@ void Context::hx(const double *d_x, double *d_y, int Bw) {
   launch_hx_assemble(fe, Ycell.p, d_y, Bw, epi, 0, stream);
   n_hx++;
   n_hx_cols += Bw;
+}
+
+// POST_PROCESS projection of v_xc to the parent mesh: distribute the child
+// constraints, evaluate v_xc + factor_lda v_LDA at the parent quadrature
+// points, and project onto the parent nodes with the GLL-lumped mass:
+// u = (C^T r) / (C^T m) on free nodes with r_i = sum_e sum_q N_i(q) f(q) JxW(q),
+// then the psi constraints distributed (hanging nodes interpolated, boundary
+// nodes zero).  The assembly already returns M^-1/2 C^T r, so one more M^-1/2
+// scaling completes the division.
+void Context::project_vxc_to_parent(const double *h_vxc, double *h_out) {
+  for (int64_t i = 0; i < ncn; ++i) check(std::isfinite(h_vxc[i]), "non-finite v_xc entry");
+  pp_pot.upload(h_vxc, (size_t)ncn, stream);
+  pp_q.ensure((size_t)nc * nq);
+  pp_y.ensure((size_t)nn);
+  launch_distribute(cchild.rows.p, cchild.ptr.p, cchild.masters.p, cchild.w.p, cchild.n, pp_pot.p, 1, stream);
+  launch_child_to_parent_quad(cv, pp_pot.p, nullptr, v_lda.p, prm.factor_lda, pp_q.p, nc * nq, stream);
+  launch_mul(pp_q.p, jxw.p, pp_q.p, nc * nq, stream);
+  launch_quad_rhs(fe, pp_q.p, Ycell.p, stream);
+  AsmEpilogue epi;
+  epi.kind = AsmEpilogue::STORE;
+  launch_hx_assemble(fe, Ycell.p, pp_y.p, 1, epi, 0, stream);
+  launch_scale_rows(invsqrtM.p, pp_y.p, pp_y.p, nn, 1, stream);
+  launch_distribute(cpsi.rows.p, cpsi.ptr.p, cpsi.masters.p, cpsi.w.p, cpsi.n, pp_y.p, 1, stream);
+  pp_y.download(h_out, (size_t)nn, stream);
+  INVDFT_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Context::evaluate_parent_field(const double *h_u, int64_t npts, const int64_t *h_cells, const double *h_xi,
+                                    double *h_out) {
+  check(npts >= 0, "negative point count");
+  for (int64_t i = 0; i < npts; ++i) {
+    check(h_cells[i] >= 0 && h_cells[i] < nc, "point cell out of range");
+    for (int d = 0; d < 3; ++d)
+      check(h_xi[3 * i + d] >= -1e-12 && h_xi[3 * i + d] <= 1.0 + 1e-12, "reference coordinate outside [0, 1]");
+  }
+  if (npts == 0) return;
+  pp_y.upload(h_u, (size_t)nn, stream);
+  pp_cells.upload(h_cells, (size_t)npts, stream);
+  pp_xi.upload(h_xi, (size_t)npts * 3, stream);
+  pp_out.ensure((size_t)npts);
+  launch_eval_points(fe, gll.p, pp_y.p, npts, pp_cells.p, pp_xi.p, pp_out.p, stream);
+  pp_out.download(h_out, (size_t)npts, stream);
+  INVDFT_CUDA(cudaStreamSynchronize(stream));
 }
 
 // Stored cell matrices back every variant but the matrix-free one, and the

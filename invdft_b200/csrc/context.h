@@ -50,7 +50,9 @@ class Context {
   // cell products: 3 matrix-free sum factorisation (default), 0 FP64 tensor core
   // on stored cell matrices (mma.sync f64), 1 row-stream DFMA, 2 bulk-staged DFMA
   int hx_variant = 3;
-  int sf_tune = 0;                 // launch shape of the matrix-free kernel
+  int sf_tune = -1;                // launch shape of the matrix-free kernel (-1: autotuned per width)
+  int sf_tuned[65];                // autotuned shape per block width (-1: not measured yet)
+  int sf_shape(const double *d_x, int Bw);
   SfMats sfm{};                    // reference-element matrices of the matrix-free variant
   DevBuf<double> vj;               // [nc][nq] v_KS * JxW (matrix-free variant)
   DevBuf<int> d_midx;              // compact numbering of the masters of hanging nodes
@@ -116,6 +118,14 @@ class Context {
   void set_params(const invdft_params *p);
   void set_subspace(const double *Xh);
   void hx(const double *d_x, double *d_y, int Bw);
+  // POST_PROCESS: child v_xc -> parent nodal field (lumped-mass L2 projection of
+  // v_xc + factor_lda v_LDA at the parent quadrature points); host arrays
+  void project_vxc_to_parent(const double *h_vxc, double *h_out);
+  // a parent nodal field at points (cell, reference coordinates); host arrays
+  void evaluate_parent_field(const double *h_u, int64_t npts, const int64_t *h_cells, const double *h_xi,
+                             double *h_out);
+  DevBuf<double> pp_pot, pp_q, pp_y, pp_xi, pp_out;   // post-processing scratch
+  DevBuf<int64_t> pp_cells;
   void set_potential_device(double *d_pot);   // distributes d_pot in place
   void lanczos_bounds(double &lo, double &hi);
   void chfsi_pass(double a, double b, double a0, std::vector<double> &res, bool low = false);

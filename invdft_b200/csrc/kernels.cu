@@ -1120,6 +1120,56 @@ __global__ void __launch_bounds__(NT) r_cell_kernel(FeView fe, const double *__r
   }
 }
 
+// Ycell[slot(e, l)] = sum_q N_l(q) fw[e*nq + q]: the cell right-hand sides of
+// an L2 projection of a quadrature field (fw = f * JxW), by sum factorisation
+// with Phi^T along the three directions.
+__global__ void __launch_bounds__(NT) quad_rhs_kernel(FeView fe, const double *__restrict__ fw,
+                                                      double *__restrict__ Ycell) {
+  extern __shared__ double sm[];
+  const int n1 = fe.n1, nd = fe.nd;
+  double *A = sm;
+  double *b0 = A + n1 * n1, *b1 = b0 + nd, *b2 = b1 + nd;
+  for (int i = threadIdx.x; i < n1 * n1; i += blockDim.x) A[i] = fe.phi[i];
+  const int64_t e = blockIdx.x;
+  for (int q = threadIdx.x; q < nd; q += blockDim.x) b0[q] = fw[e * nd + q];
+  __syncthreads();
+  tensor3(A, true, b0, b1, b2, n1, 1);
+  for (int l = threadIdx.x; l < nd; l += blockDim.x) {
+    const int sl = fe.slot_of[e * nd + l];
+    if (sl >= 0) Ycell[sl] = b1[l];
+  }
+}
+
+// out[i] = sum_l u[node(cell_i, l)] N_l(xi_i): a parent nodal field at points
+// given by their cell and reference coordinates in [0, 1]^3; the Lagrange
+// basis on the GLL nodes is evaluated on the fly.
+__global__ void eval_points_kernel(FeView fe, const double *__restrict__ gll, const double *__restrict__ u,
+                                   int64_t npts, const int64_t *__restrict__ cells,
+                                   const double *__restrict__ xi, double *__restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  const int n1 = fe.n1;
+  double l[3][kSfMaxN];
+  for (int d = 0; d < 3; ++d) {
+    const double t = xi[3 * i + d];
+    for (int a = 0; a < n1; ++a) {
+      double v = 1.0;
+      for (int b = 0; b < n1; ++b)
+        if (b != a) v *= (t - gll[b]) / (gll[a] - gll[b]);
+      l[d][a] = v;
+    }
+  }
+  const int64_t e = cells[i];
+  const int *cn = fe.cell_nodes + e * fe.nd;
+  double acc = 0.0;
+  for (int c = 0; c < n1; ++c)
+    for (int b = 0; b < n1; ++b) {
+      const double wbc = l[1][b] * l[2][c];
+      for (int a = 0; a < n1; ++a) acc = fma(l[0][a] * wbc, u[cn[a + n1 * (b + n1 * c)]], acc);
+    }
+  out[i] = acc;
+}
+
 __global__ void __launch_bounds__(NT) density_kernel(FeView fe, const double *__restrict__ psi,
                                                      const double *__restrict__ occ, int N,
                                                      const double *__restrict__ rho_t,
@@ -1368,7 +1418,7 @@ __global__ void child_to_parent_quad_kernel(ChildView cv, const double *__restri
     const double wz = (k & 4) ? z : 1.0 - z;
     v = fma(wx * wy * wz, pot[nodes[k]], v);
   }
-  vks[q] = v_base[q] + v + factor_lda * v_lda[q];
+  vks[q] = (v_base ? v_base[q] : 0.0) + v + factor_lda * v_lda[q];
 }
 
 // One CTA per work item (parent cell, range of its child cells); one warp per
@@ -1922,6 +1972,19 @@ void launch_r_cell(const FeView &fe, const double *x, const double *wq, double *
     attr = true;
   }
   r_cell_kernel<<<(unsigned)fe.nc, NT, interp_smem(fe, 0), s>>>(fe, x, wq, Ycell, B);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_quad_rhs(const FeView &fe, const double *fw, double *Ycell, cudaStream_t s) {
+  const size_t smem = sizeof(double) * ((size_t)fe.n1 * fe.n1 + 3 * (size_t)fe.nd);
+  quad_rhs_kernel<<<(unsigned)fe.nc, NT, smem, s>>>(fe, fw, Ycell);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_eval_points(const FeView &fe, const double *gll, const double *u, int64_t npts, const int64_t *cells,
+                        const double *xi, double *out, cudaStream_t s) {
+  if (npts == 0) return;
+  eval_points_kernel<<<ceil_div(npts, NT), NT, 0, s>>>(fe, gll, u, npts, cells, xi, out);
   INVDFT_LAUNCH_CHECK();
 }
 

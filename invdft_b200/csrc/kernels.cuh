@@ -132,6 +132,11 @@ void launch_pair_quad_sums(const FeView &fe, const double *Qa, const double *Qb,
 // sum_e R_e x_e with R_e = N^T diag(wq) N: Ycell [nc][nd][B]
 void launch_r_cell(const FeView &fe, const double *x, const double *wq, double *Ycell, int B,
                    cudaStream_t s);
+// cell right-hand sides of an L2 projection: Ycell[slot(e,l)] = sum_q N_l(q) fw[e,q] (width 1)
+void launch_quad_rhs(const FeView &fe, const double *fw, double *Ycell, cudaStream_t s);
+// out[i] = parent nodal field u at (cells[i], xi[3i..3i+2]) (reference coordinates in [0,1]^3)
+void launch_eval_points(const FeView &fe, const double *gll, const double *u, int64_t npts, const int64_t *cells,
+                        const double *xi, double *out, cudaStream_t s);
 // density rho = 2 sum f psi^2 at parent quad points + drho/u/loss partials
 void launch_density(const FeView &fe, const double *psi, const double *occ, int N, const double *rho_t,
                     const double *weight, const double *jxw, const double *vks, double *rho,
@@ -177,6 +182,7 @@ struct ChildView {
   const double *gll;          // [n1] parent GLL nodes
   const double *g2;           // [2] Gauss points of the child rule
 };
+// vks = v_base (optional, may be null) + child potential at parent quad points + factor_lda * v_lda
 void launch_child_to_parent_quad(const ChildView &cv, const double *pot, const double *v_base,
                                  const double *v_lda, double factor_lda, double *vks, int64_t nqtot,
                                  cudaStream_t s);

@@ -24,7 +24,7 @@ EXPORTED = [
     "invdft_set_potential", "invdft_hx", "invdft_adjoint_update_psi", "invdft_adjoint_compute_rhs",
     "invdft_adjoint_vmult", "invdft_adjoint_precondition_jacobi",
     "invdft_adjoint_precondition_jacobi_sqrt", "invdft_adjoint_distribute_x", "invdft_adjoint_solve",
-    "invdft_bfgs_solve", "invdft_coldot_noalloc",
+    "invdft_bfgs_solve", "invdft_coldot_noalloc", "invdft_project_vxc_to_parent", "invdft_evaluate_parent_field",
 ]
 
 
@@ -117,6 +117,8 @@ def load() -> C.CDLL:
         "invdft_force_backward": (C.c_int, [vp, _f64p, _P(Stats)]),
         "invdft_set_potential": (C.c_int, [vp, _f64p]),
         "invdft_hx": (C.c_int, [vp, vp, vp, C.c_int32]),
+        "invdft_project_vxc_to_parent": (C.c_int, [vp, _f64p, _f64p]),
+        "invdft_evaluate_parent_field": (C.c_int, [vp, _f64p, C.c_int64, _i64p, _f64p, _f64p]),
         "invdft_adjoint_update_psi": (C.c_int, [vp, vp, _f64p, vp, _P(C.c_int32), _P(C.c_int32),
                                                 C.c_double, _f64p, C.c_int32]),
         "invdft_adjoint_compute_rhs": (C.c_int, [vp, vp]),

@@ -17,7 +17,7 @@ import ctypes as C
 import numpy as np
 
 from . import native
-from .native import InvDFTError, Stats, f64, ptr
+from .native import InvDFTError, Stats, f64, i64, ptr
 
 
 def _check(lib, ctx, rc):
@@ -141,6 +141,27 @@ class InverseDFTSolverFunction:
     def set_potential(self, pot):
         pot = f64(pot).copy()
         _check(self.lib, self.ctx, self.lib.invdft_set_potential(self.ctx, ptr(pot)))
+
+    def project_vxc_to_parent(self, vxc_child) -> np.ndarray:
+        """POST_PROCESS projection (InverseDFTEngine::projectVxcToParentMesh,
+        InverseDFTEngine.cpp:3462-3545): the parent nodal field of v_xc +
+        factorForLDAVxc v_LDA by a lumped-mass L2 projection."""
+        v = f64(vxc_child).copy()
+        out = np.zeros(self.problem.n_nodes)
+        _check(self.lib, self.ctx, self.lib.invdft_project_vxc_to_parent(self.ctx, ptr(v), ptr(out)))
+        return out
+
+    def evaluate_parent_field(self, nodal, cells, xi) -> np.ndarray:
+        """A parent nodal field at points given by (cell, reference coordinates
+        in [0, 1]^3), as the writeToPoints branch of interpolateVxc
+        (InverseDFTEngine.cpp:3275-3456) evaluates it."""
+        u = f64(nodal)
+        c = i64(cells)
+        x = f64(xi).reshape(-1, 3)
+        out = np.zeros(c.size)
+        _check(self.lib, self.ctx, self.lib.invdft_evaluate_parent_field(self.ctx, ptr(u), c.size, ptr(c),
+                                                                         ptr(x), ptr(out)))
+        return out
 
     def hx(self, x):
         """Lowdin HX of a torch CUDA float64 block [n_nodes, B]."""

@@ -231,3 +231,33 @@ def test_mixed_precision_ladder_reaches_fp64_accuracy(name):
     assert np.max(np.abs(e - ost.eigenvalues)) < 1e-9
     assert abs(L_g - L_o) <= 1e-8 * abs(L_o)
     assert rel(f_g, f_o) < 1e-6
+
+
+@pytest.mark.parametrize("name", ["small_lih", "tiny_h2_p5"])
+def test_sf_launch_shapes_are_bitwise_identical(name, monkeypatch):
+    """The matrix-free kernel's launch shapes (one or two CTAs per SM,
+    derivative lines in registers or shared memory) run the same FMA sequence,
+    so the autotuner's choice cannot change results: HX is bitwise equal."""
+    import torch
+    from invdft_b200.solver import InverseDFTSolverFunction
+    if name == "small_lih":
+        P = problem(name)
+    else:
+        from invdft_b200.problem.system import build_problem
+        P = build_problem(name, target_solver="atoms")
+    shapes = ["0", "1"] + (["2"] if P.p == 5 else [])
+    out = {}
+    for shape in shapes + ["auto"]:
+        if shape == "auto":
+            monkeypatch.delenv("INVDFT_SF_TUNE", raising=False)
+        else:
+            monkeypatch.setenv("INVDFT_SF_TUNE", shape)
+        fn = InverseDFTSolverFunction(P, native_params())
+        fn.set_potential(P.vxc_init.copy())
+        for B in (1, 5, 16):
+            x = np.random.default_rng(100 + B).standard_normal((P.n_nodes, B))
+            out[(shape, B)] = fn.hx(torch.from_numpy(x).cuda()).cpu().numpy()
+        fn.close()
+    for shape in shapes[1:] + ["auto"]:
+        for B in (1, 5, 16):
+            assert np.array_equal(out[(shape, B)], out[("0", B)]), (shape, B)

@@ -685,6 +685,10 @@ __device__ __forceinline__ void assemble_tile_rows(const FeView &fe, const doubl
   }
 }
 
+constexpr int kAsmRow = 3;   // per-thread shares of the staged node rows (TR + 1 <= 3 NT)
+constexpr int kAsmBlk = 4;   // ... of an epilogue block (TR B <= 4 NT)
+constexpr int kAsmSeg = 8;   // ... of a staged slot segment (cap B = 2 TR B <= 8 NT)
+
 // ---------------------------------------------------------------------------
 // HX, part 2 (tiled): a CTA owns TR consecutive nodes, whose direct slots form
 // one contiguous segment [dptr[r0], dptr[r0+TR]).  The segment is streamed
@@ -693,7 +697,7 @@ __device__ __forceinline__ void assemble_tile_rows(const FeView &fe, const doubl
 // mz[midx[n]] (one load).  Thread (rr, j) handles column j of nodes r0+rr,
 // r0+rr+RR, ... (fixed order), so the MINRES dot partials are deterministic.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(NT) hx_assemble_tile_kernel(FeView fe, const double *__restrict__ Ycell,
+__global__ void __launch_bounds__(NT, 4) hx_assemble_tile_kernel(FeView fe, const double *__restrict__ Ycell,
                                                               double *__restrict__ out, int B, AsmEpilogue epi,
                                                               int TR, int cap_slots) {
   // shared layout: seg [cap][B] | s_in [TR][B] | s_prev [TR][B] | ism [TR] | dp [TR+1] | mi [TR]
@@ -711,16 +715,54 @@ __global__ void __launch_bounds__(NT) hx_assemble_tile_kernel(FeView fe, const d
   const bool need_in = epi.kind == AsmEpilogue::CHEB || epi.kind == AsmEpilogue::VMULT ||
                        epi.kind == AsmEpilogue::MINRES;
   const bool need_prev = (epi.kind == AsmEpilogue::CHEB && epi.prev) || epi.kind == AsmEpilogue::MINRES;
-  // phase A: independent coalesced loads of everything the tile reads
-  stage_copy(dp, fe.dptr + r0, rows + 1);
-  stage_copy(mi, fe.midx + r0, rows);
-  stage_copy(ism, fe.inv_sqrt_mass + r0, rows);
-  if (need_in) stage_copy(s_in, epi.in + r0 * B, rows * B);
-  if (need_prev) stage_copy(s_prev, epi.prev + r0 * B, rows * B);
-  __syncthreads();
-  const int s0 = dp[0], s1 = dp[rows];
+  // one round of loads: the slot bounds of the tile first, then every staged
+  // array into fixed per-thread register shares (the launcher keeps
+  // TR*B <= kAsmBlk*NT and 2*TR*B <= kAsmSeg*NT), then all stores
+  const int s0 = fe.dptr[r0], s1 = fe.dptr[r0 + rows];
   const bool staged = (s1 - s0) <= cap_slots;
-  if (staged) stage_copy(seg, Ycell + (int64_t)s0 * B, (s1 - s0) * B);
+  const int tid = threadIdx.x, nb = rows * B, ns = (s1 - s0) * B;
+  int v_dp[kAsmRow], v_mi[kAsmRow];
+  double v_ism[kAsmRow], v_in[kAsmBlk], v_pr[kAsmBlk], v_sg[kAsmSeg];
+#pragma unroll
+  for (int u = 0; u < kAsmRow; ++u) {
+    const int i = tid + u * NT;
+    v_dp[u] = i <= rows ? fe.dptr[r0 + i] : 0;
+    v_mi[u] = i < rows ? fe.midx[r0 + i] : -1;
+    v_ism[u] = i < rows ? fe.inv_sqrt_mass[r0 + i] : 0.0;
+  }
+#pragma unroll
+  for (int u = 0; u < kAsmBlk; ++u) {
+    const int i = tid + u * NT;
+    v_in[u] = (need_in && i < nb) ? epi.in[r0 * B + i] : 0.0;
+    v_pr[u] = (need_prev && i < nb) ? epi.prev[r0 * B + i] : 0.0;
+  }
+#pragma unroll
+  for (int u = 0; u < kAsmSeg; ++u) {
+    const int i = tid + u * NT;
+    v_sg[u] = (staged && i < ns) ? Ycell[(int64_t)s0 * B + i] : 0.0;
+  }
+#pragma unroll
+  for (int u = 0; u < kAsmRow; ++u) {
+    const int i = tid + u * NT;
+    if (i <= rows) dp[i] = v_dp[u];
+    if (i < rows) {
+      mi[i] = v_mi[u];
+      ism[i] = v_ism[u];
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kAsmBlk; ++u) {
+    const int i = tid + u * NT;
+    if (i < nb) {
+      if (need_in) s_in[i] = v_in[u];
+      if (need_prev) s_prev[i] = v_pr[u];
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kAsmSeg; ++u) {
+    const int i = tid + u * NT;
+    if (staged && i < ns) seg[i] = v_sg[u];
+  }
   __syncthreads();
   double dot = 0.0;
   assemble_tile_rows(fe, staged ? seg : Ycell, staged ? (int64_t)s0 * B : 0, dp, mi, ism, s_in, s_prev, r0, rows,
@@ -1848,6 +1890,8 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
   }
   int TR, cap;
   assemble_shape(B, TR, cap);
+  if (TR + 1 > kAsmRow * NT || TR * B > kAsmBlk * NT || cap * B > kAsmSeg * NT)
+    throw StatusError(5, "assembly tile larger than its staging shares");
   const int nb = (int)((fe.nnodes + TR - 1) / TR);   // one tile of TR nodes per CTA
   if (fe.nhang > 0) {
     hanging_sum_kernel<<<ceil_div((int64_t)fe.nhang * B, NT), NT, 0, s>>>(fe, Ycell, B);

@@ -158,7 +158,9 @@ void build_slots(int64_t nrows, int64_t ncell, int per_cell, const int64_t *cell
 // compact index and list of partial rows, in group order.
 struct ConsGroups {
   std::vector<int> rptr{0}, rows, hrow, m0, nm, poff, midx, mp_ptr{0}, mp_idx;
+  std::vector<int64_t> woff;     // start of each group's [row][master] weight block
   int ngroup = 0, ngroup_h = 0, maxnm = 0, maxnr = 0, nmast = 0, npairs = 0;
+  int64_t nw = 0;
 };
 
 ConsGroups build_groups(int64_t nrows, const invdft_constraints &c) {
@@ -185,6 +187,8 @@ ConsGroups build_groups(int64_t nrows, const invdft_constraints &c) {
       G.hrow.push_back(hidx[L[q]]);
     }
     G.rptr.push_back((int)G.rows.size());
+    G.woff.push_back(G.nw);
+    G.nw += (int64_t)(b - a) * nm;
     G.m0.push_back(m0);
     G.nm.push_back(nm);
     G.poff.push_back(G.npairs);
@@ -378,8 +382,27 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
     d_mp_idx.upload(G.mp_idx, s);
     d_mz.alloc((size_t)std::max(G.nmast, 1) * 64);
     d_gpart.alloc((size_t)std::max(G.npairs, 1) * 64);
+    {
+      // weights of each group's rows laid out contiguously, [row][master]
+      std::vector<double> gw(std::max<int64_t>(G.nw, 1), 0.0), w(std::max<int64_t>(G.nw, 1), 0.0);
+      for (int g = 0; g < G.ngroup; ++g)
+        for (int q = G.rptr[g]; q < G.rptr[g + 1]; ++q) {
+          const int64_t base = d->cons_psi.ptr[G.rows[q]];
+          const int64_t o = G.woff[g] + (int64_t)(q - G.rptr[g]) * G.nm[g];
+          for (int t = 0; t < G.nm[g]; ++t) {
+            gw[o + t] = cgw[base + t];
+            w[o + t] = d->cons_psi.weights[base + t];
+          }
+        }
+      d_g_woff.upload(G.woff.empty() ? std::vector<int64_t>{0} : G.woff, s);
+      d_g_gw.upload(gw, s);
+      d_g_w.upload(w, s);
+    }
     fe.ngroup = G.ngroup; fe.ngroup_h = G.ngroup_h; fe.g_maxnm = G.maxnm; fe.g_maxnr = G.maxnr;
-    check((size_t)std::max(G.maxnm, 1) * (64 + kGroupRows) * 8 <= 200 * 1024, "a constraint row has too many masters");
+    // INVDFT_GROUP_STAGE (doubles, diagnostics) lowers the shared staging of a
+    // constraint group; groups that do not fit read global memory instead
+    const char *gs = std::getenv("INVDFT_GROUP_STAGE");
+    fe.g_stage = gs ? std::max(0, std::min(std::atoi(gs), kGroupStage)) : kGroupStage;
   }
   d_zptr.upload(zptr_h, s);
   d_z.alloc((size_t)std::max(nhang, 1) * 64);
@@ -436,6 +459,7 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   fe.g_rptr = d_g_rptr.p; fe.g_rows = d_g_rows.p; fe.g_hrow = d_g_hrow.p; fe.g_m0 = d_g_m0.p;
   fe.g_nm = d_g_nm.p; fe.g_poff = d_g_poff.p; fe.mp_ptr = d_mp_ptr.p; fe.mp_idx = d_mp_idx.p;
   fe.gpart = d_gpart.p;
+  fe.g_woff = d_g_woff.p; fe.g_gw = d_g_gw.p; fe.g_w = d_g_w.p;
   d_hvg.alloc((size_t)std::max(cpsi.n, 1) * 64);
   fe.hvg = d_hvg.p;
   fe.err = d_err.p;

@@ -61,6 +61,8 @@ class Context {
   // constraint groups (rows with identical master lists) and master pair lists
   DevBuf<int> d_g_rptr, d_g_rows, d_g_hrow, d_g_m0, d_g_nm, d_g_poff, d_mp_ptr, d_mp_idx;
   DevBuf<double> d_gpart;          // [npairs][64] per-(group, master) partial sums
+  DevBuf<int64_t> d_g_woff;        // per-group start of its weight block
+  DevBuf<double> d_g_gw, d_g_w;    // group weights, Lowdin-scaled and plain
   DevBuf<double> d_hvg;            // [ncons][64] pre-gathered constrained rows (matrix-free variant)
   bool needs_cell_matrices() const;
   void check_device_error();

@@ -928,21 +928,28 @@ __global__ void hanging_sum_kernel(FeView fe, const double *__restrict__ Ycell, 
 // and writes gpart[g_poff[g] + t][j] = sum_q w[row q, t] z[row q][j] for each
 // of its masters t; then mz[i][j] sums master i's (group, master) partials,
 // both in a fixed order.
-__global__ void __launch_bounds__(NT) group_partial_kernel(FeView fe, int B) {
+__global__ void __launch_bounds__(NT) group_partial_kernel(FeView fe, int B, int cap) {
   extern __shared__ double sp[];   // zr [nr][B] | wm [nr][nm]
   const int g = blockIdx.x;
   const int nm = fe.g_nm[g], rp0 = fe.g_rptr[g], nr = fe.g_rptr[g + 1] - rp0;
+  const int64_t po = fe.g_poff[g];
+  const double *w = fe.g_w + fe.g_woff[g];
+  if ((int64_t)nr * (B + nm) > cap) {   // too large to stage: read from global memory
+    for (int i = threadIdx.x; i < nm * B; i += blockDim.x) {
+      const int t = i / B, j = i - t * B;
+      double acc = 0.0;
+      for (int q = 0; q < nr; ++q) acc = fma(w[q * nm + t], fe.z[(int64_t)fe.g_hrow[rp0 + q] * B + j], acc);
+      fe.gpart[(po + t) * B + j] = acc;
+    }
+    return;
+  }
   double *zr = sp, *wm = sp + (size_t)nr * B;
   for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
     const int q = i / B, j = i - q * B;
     zr[i] = fe.z[(int64_t)fe.g_hrow[rp0 + q] * B + j];
   }
-  for (int i = threadIdx.x; i < nr * nm; i += blockDim.x) {
-    const int q = i / nm, t = i - q * nm;
-    wm[i] = fe.cons_w[fe.cons_ptr[fe.g_rows[rp0 + q]] + t];
-  }
+  for (int i = threadIdx.x; i < nr * nm; i += blockDim.x) wm[i] = w[i];
   __syncthreads();
-  const int64_t po = fe.g_poff[g];
   for (int i = threadIdx.x; i < nm * B; i += blockDim.x) {
     const int t = i / B, j = i - t * B;
     double acc = 0.0;
@@ -1684,20 +1691,30 @@ void launch_hx_cell_dmma_f32(const FeView &fe, const float *H32, const double *x
 // FMA order of gather_value, so the matrix-free kernel reads each with one
 // load.  One CTA per constraint group: the group's master rows and weights
 // are read once into shared memory and serve all of its rows.
-__global__ void __launch_bounds__(NT) group_gather_kernel(FeView fe, const double *__restrict__ x, int B) {
+__global__ void __launch_bounds__(NT) group_gather_kernel(FeView fe, const double *__restrict__ x, int B,
+                                                          int cap) {
   extern __shared__ double sg[];   // xm [nm][B] | wm [nr][nm]
   const int g = blockIdx.x;
   const int nm = fe.g_nm[g], m0 = fe.g_m0[g];
   const int rp0 = fe.g_rptr[g], nr = fe.g_rptr[g + 1] - rp0;
+  const double *gw = fe.g_gw + fe.g_woff[g];
+  if ((int64_t)nm * (B + nr) > cap) {
+    // a group too large for the shared staging (rows with hundreds of masters
+    // after constraint closure): the same sums, read from global memory
+    for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
+      const int q = i / B, j = i - q * B;
+      double v = 0.0;
+      for (int t = 0; t < nm; ++t) v = fma(gw[q * nm + t], x[(int64_t)fe.cons_masters[m0 + t] * B + j], v);
+      fe.hvg[(int64_t)fe.g_rows[rp0 + q] * B + j] = v;
+    }
+    return;
+  }
   double *xm = sg, *wm = sg + (size_t)nm * B;
   for (int i = threadIdx.x; i < nm * B; i += blockDim.x) {
     const int t = i / B, j = i - t * B;
     xm[i] = x[(int64_t)fe.cons_masters[m0 + t] * B + j];
   }
-  for (int i = threadIdx.x; i < nr * nm; i += blockDim.x) {
-    const int q = i / nm, t = i - q * nm;
-    wm[i] = fe.cons_gw[fe.cons_ptr[fe.g_rows[rp0 + q]] + t];
-  }
+  for (int i = threadIdx.x; i < nr * nm; i += blockDim.x) wm[i] = gw[i];
   __syncthreads();
   for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
     const int q = i / B, j = i - q * B;
@@ -1745,13 +1762,14 @@ static void hx_sf_dispatch(const FeView &fe, const SfMats &mt, const double *vj,
 void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell,
                        int B, int gather_mode, int tune, cudaStream_t s) {
   if (gather_mode != GATHER_PLAIN && fe.ngroup > 0) {
-    const size_t smem = sizeof(double) * (size_t)std::max(fe.g_maxnm, 1) * (B + fe.g_maxnr);
+    // staging capacity: the largest group's need, at most fe.g_stage doubles
+    const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnm, 1) * (B + fe.g_maxnr), fe.g_stage);
     static bool attr = false;
     if (!attr) {
       INVDFT_CUDA(cudaFuncSetAttribute(group_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
       attr = true;
     }
-    group_gather_kernel<<<fe.ngroup, NT, smem, s>>>(fe, x, B);
+    group_gather_kernel<<<fe.ngroup, NT, sizeof(double) * (size_t)cap, s>>>(fe, x, B, cap);
     INVDFT_LAUNCH_CHECK();
   }
   if (tune == 2 && fe.n1 == 6) {   // two CTAs per SM, derivative lines in shared memory
@@ -1898,13 +1916,14 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
     INVDFT_LAUNCH_CHECK();
   }
   if (fe.nmast > 0) {
-    const size_t smem = sizeof(double) * (size_t)std::max(fe.g_maxnr, 1) * (B + std::max(fe.g_maxnm, 1));
+    const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnr, 1) * (B + std::max(fe.g_maxnm, 1)),
+                                           fe.g_stage);
     static bool attr = false;
     if (!attr) {
       INVDFT_CUDA(cudaFuncSetAttribute(group_partial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
       attr = true;
     }
-    group_partial_kernel<<<fe.ngroup_h, NT, smem, s>>>(fe, B);
+    group_partial_kernel<<<fe.ngroup_h, NT, sizeof(double) * (size_t)cap, s>>>(fe, B, cap);
     INVDFT_LAUNCH_CHECK();
     master_sum_kernel<<<ceil_div((int64_t)fe.nmast * B, NT), NT, 0, s>>>(fe, B);
     INVDFT_LAUNCH_CHECK();

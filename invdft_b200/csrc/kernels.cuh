@@ -39,7 +39,12 @@ struct FeView {
   // (g, t) of a hanging group is partial row g_poff[g] + t; master i sums the
   // partial rows mp_idx[mp_ptr[i] .. mp_ptr[i+1]).
   int ngroup, ngroup_h, g_maxnm, g_maxnr;
+  int g_stage;              // shared staging per group, doubles; larger groups read global memory
   const int *g_rptr, *g_rows, *g_hrow, *g_m0, *g_nm, *g_poff;
+  // the weights of group g's rows, [row q][master t] contiguous from g_woff[g]:
+  // Lowdin-scaled (gw, for the gather) and plain (w, for the transpose)
+  const int64_t *g_woff;
+  const double *g_gw, *g_w;
   const int *mp_ptr, *mp_idx;
   double *gpart;            // [npairs][B] scratch: per (group, master) partial sums
   double *hvg;              // [ncons][B] scratch: Lowdin-gathered values of the constrained rows
@@ -47,7 +52,8 @@ struct FeView {
   const double *inv_sqrt_mass, *sqrt_mass;
 };
 
-constexpr int kGroupRows = 64;   // constraint rows per group at most
+constexpr int kGroupRows = 64;     // constraint rows per group at most
+constexpr int kGroupStage = 12288; // default shared staging per constraint group (96 KB of doubles)
 
 // Gather modes of the cell GEMM.
 enum GatherMode { GATHER_LOWDIN = 0, GATHER_PLAIN = 1 };

@@ -72,6 +72,36 @@ def test_hx_cell_variants_match_oracle(name, variant, monkeypatch):
         assert rel(y, orc.ops.hx(x)) < TOL_OP, (variant, B)
 
 
+@pytest.mark.parametrize("name", ["small_lih", "tiny_h2_p5"])
+def test_hx_with_unstaged_constraint_groups(name, monkeypatch):
+    """Constraint groups too large for their shared-memory staging (rows with
+    hundreds of masters after closure, as on the largest meshes) take a
+    global-memory path with the same sums: with the staging forced to zero,
+    every group takes it and HX still matches the oracle."""
+    import torch
+    from invdft_b200.solver import InverseDFTSolverFunction
+    from oracle import InverseDFTSolverFunction as Oracle
+    from oracle.fe import child_to_parent_quad
+    monkeypatch.setenv("INVDFT_GROUP_STAGE", "0")
+    if name == "small_lih":
+        P = problem(name)
+    else:
+        from invdft_b200.problem.system import build_problem
+        P = build_problem(name, target_solver="atoms")
+    fn = InverseDFTSolverFunction(P, native_params())
+    orc = Oracle(P, oracle_params())
+    pot = P.vxc_init.copy()
+    fn.set_potential(pot)
+    orc.ops.cell_hamiltonians(P.v_base + child_to_parent_quad(P, pot))
+    rng = np.random.default_rng(13)
+    for B in (1, 7, 16):
+        x = rng.standard_normal((P.n_nodes, B))
+        x[~orc.free] = 0.0
+        y = fn.hx(torch.from_numpy(x).cuda()).cpu().numpy()
+        assert rel(y, orc.ops.hx(x)) < TOL_OP, B
+    fn.close()
+
+
 @pytest.mark.parametrize("name", ["tiny_h2", "small_lih"])
 def test_eigensolve_and_density(name):
     P, fn, orc = _pair(name)

@@ -304,6 +304,24 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
       }
       sfm.w[q] = gq[q];
     }
+    if (n1 % 2 == 0) {
+      // even-odd halves (the node and point sets are symmetric about 1/2)
+      const int h = n1 / 2;
+      auto M = [&](const double *X, int q, int a) { return X[q * n1 + a]; };
+      for (int q = 0; q < h; ++q)
+        for (int a = 0; a < h; ++a) {
+          const int k = q * h + a;
+          sfm.phe[k] = 0.5 * (M(sfm.phi, q, a) + M(sfm.phi, q, n1 - 1 - a));
+          sfm.pho[k] = 0.5 * (M(sfm.phi, q, a) - M(sfm.phi, q, n1 - 1 - a));
+          sfm.dqe[k] = 0.5 * (M(sfm.dq, q, a) + M(sfm.dq, q, n1 - 1 - a));
+          sfm.dqo[k] = 0.5 * (M(sfm.dq, q, a) - M(sfm.dq, q, n1 - 1 - a));
+          // transposes: row q of X^T is column q of X
+          sfm.pte[k] = 0.5 * (M(sfm.phi, a, q) + M(sfm.phi, n1 - 1 - a, q));
+          sfm.pto[k] = 0.5 * (M(sfm.phi, a, q) - M(sfm.phi, n1 - 1 - a, q));
+          sfm.dte[k] = 0.5 * (M(sfm.dq, a, q) + M(sfm.dq, n1 - 1 - a, q));
+          sfm.dto[k] = 0.5 * (M(sfm.dq, a, q) - M(sfm.dq, n1 - 1 - a, q));
+        }
+    }
   }
   std::vector<double> w3(nd);
   for (int i = 0; i < nd; ++i) w3[i] = gw[i % n1] * gw[(i / n1) % n1] * gw[i / (n1 * n1)];
@@ -610,9 +628,11 @@ void Context::cell_gemm(const double *d_x, int Bw, bool low) {
     ev_used += 2;
     if (!low && hx_variant == 3) {
       // algorithmic traffic: the block once, v JxW once, the cell results once;
-      // 12 n1^4 FMAs per (cell, column)
+      // work: 12 1D applications on n1^2 lines per (cell, column), each n1^2
+      // FMAs, or n1^2/2 FMAs + 2 n1 adds in even-odd form (even n1)
       prof_bytes += 8.0 * ((double)nn * Bw + (double)nc * nq + (double)nc * nd * Bw);
-      prof_flops += 24.0 * (double)nc * nd * n1 * Bw;
+      const double per_line = (n1 % 2 == 0) ? (double)n1 * n1 + 2.0 * n1 : 2.0 * n1 * n1;
+      prof_flops += 12.0 * (double)nc * n1 * n1 * per_line * Bw;
     } else {
       // algorithmic traffic: cell matrices once, the block once, the cell results once
       prof_bytes += (low ? 4.0 : 8.0) * (double)nc * nd * nd + 8.0 * ((double)nn * Bw + (double)nc * nd * Bw);

@@ -77,10 +77,19 @@ void launch_narrow(const double *src, float *dst, int64_t n, cudaStream_t s);
 // dq[q*n1+r] = derivative at g_q of the Lagrange basis on the Gauss points,
 // w = 1D Gauss weights on [0, 1].
 constexpr int kSfMaxN = 8;
+constexpr int kSfMaxH = kSfMaxN / 2;
 struct SfMats {
   double phi[kSfMaxN * kSfMaxN];
   double dq[kSfMaxN * kSfMaxN];
   double w[kSfMaxN];
+  // even n1: even-odd halves [q*h + a] (h = n1/2) of the four 1D operators,
+  // applied as out[q] = E + O, out[n1-1-q] = E - O (Phi, Phi^T: centro-
+  // symmetric) or O - E (Dq, Dq^T: centro-antisymmetric), with
+  // E = sum_a Xe[q][a] (in[a] + in[n1-1-a]), O = sum_a Xo[q][a] (in[a] - in[n1-1-a])
+  double phe[kSfMaxH * kSfMaxH], pho[kSfMaxH * kSfMaxH];   // Phi
+  double dqe[kSfMaxH * kSfMaxH], dqo[kSfMaxH * kSfMaxH];   // Dq
+  double pte[kSfMaxH * kSfMaxH], pto[kSfMaxH * kSfMaxH];   // Phi^T
+  double dte[kSfMaxH * kSfMaxH], dto[kSfMaxH * kSfMaxH];   // Dq^T
 };
 // matrix-free variant: vj [nc][nq] = v_KS * JxW at the parent quadrature points;
 // tune 0: one CTA per SM allowed the registers it wants, 1: two CTAs per SM,

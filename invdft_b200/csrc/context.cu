@@ -322,6 +322,7 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
           sfm.dto[k] = 0.5 * (M(sfm.dq, a, q) - M(sfm.dq, n1 - 1 - a, q));
         }
     }
+    sfm32 = sfm.as<float>();
   }
   std::vector<double> w3(nd);
   for (int i = 0; i < nd; ++i) w3[i] = gw[i % n1] * gw[(i / n1) % n1] * gw[i / (n1 * n1)];
@@ -618,7 +619,8 @@ void Context::cell_gemm(const double *d_x, int Bw, bool low) {
   const int shape = (!low && hx_variant == 3) ? sf_shape(d_x, Bw) : 0;   // tuning stays outside the timing
   const bool rec = profile && ev_used + 2 <= (int)ev_pool.size();
   if (rec) INVDFT_CUDA(cudaEventRecord(ev_pool[ev_used], stream));
-  if (low) launch_hx_cell_dmma_f32(fe, H32.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
+  if (low && hx_variant == 3) launch_hx_cell_sf_f32(fe, sfm32, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
+  else if (low) launch_hx_cell_dmma_f32(fe, H32.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
   else if (hx_variant == 3) launch_hx_cell_sf(fe, sfm, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, shape, stream);
   else if (hx_variant == 0) launch_hx_cell_dmma(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
   else if (hx_variant == 2) launch_hx_cell_gemm_bulk(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
@@ -626,7 +628,7 @@ void Context::cell_gemm(const double *d_x, int Bw, bool low) {
   if (rec) {
     INVDFT_CUDA(cudaEventRecord(ev_pool[ev_used + 1], stream));
     ev_used += 2;
-    if (!low && hx_variant == 3) {
+    if (hx_variant == 3) {
       // algorithmic traffic: the block once, v JxW once, the cell results once;
       // work: 12 1D applications on n1^2 lines per (cell, column), each n1^2
       // FMAs, or n1^2/2 FMAs + 2 n1 adds in even-odd form (even n1)
@@ -719,10 +721,10 @@ void Context::evaluate_parent_field(const double *h_u, int64_t npts, const int64
   INVDFT_CUDA(cudaStreamSynchronize(stream));
 }
 
-// Stored cell matrices back every variant but the matrix-free one, and the
-// FP32-stored filter of the mixed-precision ladder.
+// Stored cell matrices back every variant but the matrix-free one (whose low
+// rungs run the FP32 matrix-free kernel instead of FP32-stored matrices).
 bool Context::needs_cell_matrices() const {
-  return hx_variant != 3 || prm.precision == INVDFT_PRECISION_MIXED;
+  return hx_variant != 3;
 }
 
 void Context::set_potential_device(double *d_pot) {
@@ -737,7 +739,7 @@ void Context::set_potential_device(double *d_pot) {
   }
   have_H = true;
   have_H32 = false;
-  if (prm.precision == INVDFT_PRECISION_MIXED) {
+  if (prm.precision == INVDFT_PRECISION_MIXED && needs_cell_matrices()) {
     H32.ensure(H.n);
     launch_narrow(H.p, H32.p, (int64_t)H.n, stream);
     have_H32 = true;
@@ -917,10 +919,11 @@ void Context::solve_eigen(double *d_pot, invdft_force_stats *st) {
   int passes = 0, passes_low = 0;
   double maxres = 0.0, prev_maxres = 1e300;
   std::vector<double> res;
-  // precision ladder: filter with the FP32-stored cell matrices while the
+  // precision ladder: filter in FP32 (the FP32 matrix-free kernel, or
+  // FP32-stored cell matrices for the stored-matrix variants) while the
   // residual keeps falling and stays above the floor, then finish in FP64
   // (Rayleigh-Ritz and the residual norms are always FP64)
-  bool low = prm.precision == INVDFT_PRECISION_MIXED && have_H32;
+  bool low = prm.precision == INVDFT_PRECISION_MIXED && (hx_variant == 3 || have_H32);
   for (;;) {
     double a, a0;
     if (!have_eig) {

@@ -54,6 +54,7 @@ class Context {
   int sf_tuned[65];                // autotuned shape per block width (-1: not measured yet)
   int sf_shape(const double *d_x, int Bw);
   SfMats sfm{};                    // reference-element matrices of the matrix-free variant
+  SfMatsT<float> sfm32{};          // the same in FP32 (low rungs of the precision ladder)
   DevBuf<double> vj;               // [nc][nq] v_KS * JxW (matrix-free variant)
   DevBuf<int> d_midx;              // compact numbering of the masters of hanging nodes
   DevBuf<double> d_mz;             // [nmast][64] per-master hanging contributions

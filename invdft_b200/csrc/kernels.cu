@@ -339,45 +339,48 @@ __device__ __forceinline__ int sf_point(int L, int k) {
   return L + N * N * k;                                        // z-line, L = i + N j
 }
 
-template <int N, int DIR>
-__device__ __forceinline__ void sf_load(const double *a, int L, int p, double (&r)[N]) {
+__device__ __forceinline__ double sf_fma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float sf_fma(float a, float b, float c) { return fmaf(a, b, c); }
+
+template <int N, int DIR, typename T>
+__device__ __forceinline__ void sf_load(const T *a, int L, int p, T (&r)[N]) {
 #pragma unroll
   for (int k = 0; k < N; ++k) r[k] = a[sf_point<N, DIR>(L, k) * 16 + p];
 }
-template <int N, int DIR>
-__device__ __forceinline__ void sf_store(double *a, int L, int p, const double (&r)[N]) {
+template <int N, int DIR, typename T>
+__device__ __forceinline__ void sf_store(T *a, int L, int p, const T (&r)[N]) {
 #pragma unroll
   for (int k = 0; k < N; ++k) a[sf_point<N, DIR>(L, k) * 16 + p] = r[k];
 }
 // out[q] = sum_a M[q][a] in[a]  (M row-major N x N)
-template <int N>
-__device__ __forceinline__ void sf_apply(const double *M, const double (&in)[N], double (&out)[N]) {
+template <int N, typename T>
+__device__ __forceinline__ void sf_apply(const T *M, const T (&in)[N], T (&out)[N]) {
 #pragma unroll
   for (int q = 0; q < N; ++q) {
-    double s = 0.0;
+    T s = T(0);
 #pragma unroll
-    for (int a = 0; a < N; ++a) s = fma(M[q * N + a], in[a], s);
+    for (int a = 0; a < N; ++a) s = sf_fma(M[q * N + a], in[a], s);
     out[q] = s;
   }
 }
 // out[a] += sum_q M[q][a] in[q]
-template <int N>
-__device__ __forceinline__ void sf_apply_t(const double *M, const double (&in)[N], double (&out)[N]) {
+template <int N, typename T>
+__device__ __forceinline__ void sf_apply_t(const T *M, const T (&in)[N], T (&out)[N]) {
 #pragma unroll
   for (int a = 0; a < N; ++a) {
-    double s = out[a];
+    T s = out[a];
 #pragma unroll
-    for (int q = 0; q < N; ++q) s = fma(M[q * N + a], in[q], s);
+    for (int q = 0; q < N; ++q) s = sf_fma(M[q * N + a], in[q], s);
     out[a] = s;
   }
 }
 
 // Even-odd application of a centro-symmetric (ANTI: centro-antisymmetric) 1D
 // operator from its halves: 2 (N/2)^2 FMAs instead of N^2.  ACC adds into out.
-template <int N, bool ANTI, bool ACC>
-__device__ __forceinline__ void sf_eo(const double *Xe, const double *Xo, const double (&in)[N], double (&out)[N]) {
+template <int N, bool ANTI, bool ACC, typename T>
+__device__ __forceinline__ void sf_eo(const T *Xe, const T *Xo, const T (&in)[N], T (&out)[N]) {
   constexpr int H = N / 2;
-  double e[H], o[H];
+  T e[H], o[H];
 #pragma unroll
   for (int a = 0; a < H; ++a) {
     e[a] = in[a] + in[N - 1 - a];
@@ -385,69 +388,73 @@ __device__ __forceinline__ void sf_eo(const double *Xe, const double *Xo, const 
   }
 #pragma unroll
   for (int q = 0; q < H; ++q) {
-    double E = 0.0, O = 0.0;
+    T E = T(0), O = T(0);
 #pragma unroll
     for (int a = 0; a < H; ++a) {
-      E = fma(Xe[q * H + a], e[a], E);
-      O = fma(Xo[q * H + a], o[a], O);
+      E = sf_fma(Xe[q * H + a], e[a], E);
+      O = sf_fma(Xo[q * H + a], o[a], O);
     }
-    const double lo = E + O, hi = ANTI ? O - E : E - O;
+    const T lo = E + O, hi = ANTI ? O - E : E - O;
     out[q] = ACC ? out[q] + lo : lo;
     out[N - 1 - q] = ACC ? out[N - 1 - q] + hi : hi;
   }
 }
 // The four 1D operators of the cell product: even orders of N use the
 // even-odd halves, odd N the full matrices.
-template <int N>
-__device__ __forceinline__ void sf_phi(const SfMats &mt, const double (&in)[N], double (&out)[N]) {
+template <int N, typename T>
+__device__ __forceinline__ void sf_phi(const SfMatsT<T> &mt, const T (&in)[N], T (&out)[N]) {
   if constexpr (N % 2 == 0) sf_eo<N, false, false>(mt.phe, mt.pho, in, out);
   else sf_apply<N>(mt.phi, in, out);
 }
-template <int N>
-__device__ __forceinline__ void sf_dq(const SfMats &mt, const double (&in)[N], double (&out)[N]) {
+template <int N, typename T>
+__device__ __forceinline__ void sf_dq(const SfMatsT<T> &mt, const T (&in)[N], T (&out)[N]) {
   if constexpr (N % 2 == 0) sf_eo<N, true, false>(mt.dqe, mt.dqo, in, out);
   else sf_apply<N>(mt.dq, in, out);
 }
-template <int N>   // out += Dq^T in
-__device__ __forceinline__ void sf_dqt_add(const SfMats &mt, const double (&in)[N], double (&out)[N]) {
+template <int N, typename T>   // out += Dq^T in
+__device__ __forceinline__ void sf_dqt_add(const SfMatsT<T> &mt, const T (&in)[N], T (&out)[N]) {
   if constexpr (N % 2 == 0) sf_eo<N, true, true>(mt.dte, mt.dto, in, out);
   else sf_apply_t<N>(mt.dq, in, out);
 }
-template <int N>   // out = Phi^T in
-__device__ __forceinline__ void sf_phit(const SfMats &mt, const double (&in)[N], double (&out)[N]) {
+template <int N, typename T>   // out = Phi^T in
+__device__ __forceinline__ void sf_phit(const SfMatsT<T> &mt, const T (&in)[N], T (&out)[N]) {
   if constexpr (N % 2 == 0) {
     sf_eo<N, false, false>(mt.pte, mt.pto, in, out);
   } else {
 #pragma unroll
-    for (int a = 0; a < N; ++a) out[a] = 0.0;
+    for (int a = 0; a < N; ++a) out[a] = T(0);
     sf_apply_t<N>(mt.phi, in, out);
   }
 }
 
-template <int N, int MINB, bool GXS>
-__global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe, SfMats mt, const double *__restrict__ vj,
+template <int N, int MINB, bool GXS, typename T = double>
+__global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe, SfMatsT<T> mt, const double *__restrict__ vj,
                                                                 const double *__restrict__ x,
                                                                 double *__restrict__ Ycell, int B, int C, int mode) {
   // GXS: the weighted x-derivative lines wait in a fourth shared array instead
-  // of registers between the forward and the backward x pass
+  // of registers between the forward and the backward x pass.  T is the
+  // arithmetic type (double; float for the low rungs of the precision ladder):
+  // the gathered values and v JxW are rounded to T, the results widened to
+  // double in the cell-result slots.
   constexpr int N2 = N * N, N3 = N2 * N;
-  extern __shared__ double sm[];
-  double *A = sm, *Bs = sm + N3 * 16, *Cs = sm + 2 * N3 * 16, *Gs = sm + 3 * N3 * 16;
+  extern __shared__ __align__(16) unsigned char sf_smem[];
+  T *sm = reinterpret_cast<T *>(sf_smem);
+  T *A = sm, *Bs = sm + N3 * 16, *Cs = sm + 2 * N3 * 16, *Gs = sm + 3 * N3 * 16;
   const int p = threadIdx.x & 15, L = threadIdx.x >> 4;
   const int G = 16 / C;
   const int g = p / C, c = p - g * C;
   const int64_t e = (int64_t)blockIdx.x * G + g;
   const int b = blockIdx.y * C + c;
   const bool act = e < fe.nc && b < B;
-  const double hh = act ? 0.5 * fe.cell_h[e] : 0.0;
-  double wa = 0.0, wb = 0.0;   // weights of the two coordinates off the line (compile-time indices)
+  const T hh = act ? T(0.5 * fe.cell_h[e]) : T(0);
+  T wa = T(0), wb = T(0);   // weights of the two coordinates off the line (compile-time indices)
 #pragma unroll
   for (int k = 0; k < N; ++k) {
     if (L % N == k) wa = mt.w[k];
     if (L / N == k) wb = mt.w[k];
   }
-  const double f = hh * wa * wb;
-  double r[N], s[N], gx[N];
+  const T f = hh * wa * wb;
+  T r[N], s[N], gx[N];
   // gather of the z-line L straight into registers: all N node indices, then
   // all 2N independent value loads, then the (rare) hanging rows; phi along z
   {
@@ -462,11 +469,11 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
       const bool direct = act && m[k] >= 0;
       const double xv = direct ? x[(int64_t)m[k] * B + b] : 0.0;
       const double sc = (direct && mode != GATHER_PLAIN) ? fe.inv_sqrt_mass[m[k]] : 1.0;
-      r[k] = xv * sc;
+      r[k] = T(xv * sc);
     }
 #pragma unroll
     for (int k = 0; k < N; ++k)   // constrained rows: pre-gathered by hanging_gather_kernel
-      if (act && m[k] < 0) r[k] = fe.hvg[(int64_t)(-m[k] - 1) * B + b];
+      if (act && m[k] < 0) r[k] = T(fe.hvg[(int64_t)(-m[k] - 1) * B + b]);
   }
   sf_phi<N>(mt, r, s);
   sf_store<N, 2>(A, L, p, s);
@@ -489,9 +496,9 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
   for (int q = 0; q < N; ++q) s[q] *= f * mt.w[q];
   sf_store<N, 1>(Cs, L, p, s);
   {
-    double v[N];
+    T v[N];
 #pragma unroll
-    for (int k = 0; k < N; ++k) v[k] = act ? vj[e * N3 + L + N2 * k] : 0.0;
+    for (int k = 0; k < N; ++k) v[k] = act ? T(vj[e * N3 + L + N2 * k]) : T(0);
     sf_load<N, 2>(A, L, p, r);           // d/dz, the z back pass and the potential term
     sf_dq<N>(mt, r, s);
 #pragma unroll
@@ -524,7 +531,7 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
 #pragma unroll
     for (int k = 0; k < N; ++k) {
       const int sl = fe.slot_of[e * N3 + L + N2 * k];
-      if (sl >= 0) Ycell[(int64_t)sl * B + b] = s[k];
+      if (sl >= 0) Ycell[(int64_t)sl * B + b] = double(s[k]);
     }
   }
 }
@@ -1770,14 +1777,14 @@ __global__ void __launch_bounds__(NT) group_gather_kernel(FeView fe, const doubl
   }
 }
 
-template <int N, int MINB, bool GXS = false>
-static void hx_sf_n(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell, int B,
+template <int N, int MINB, bool GXS = false, typename T = double>
+static void hx_sf_n(const FeView &fe, const SfMatsT<T> &mt, const double *vj, const double *x, double *Ycell, int B,
                     int mode, cudaStream_t s) {
   constexpr int threads = 16 * N * N;
-  const size_t smem = sizeof(double) * (GXS ? 4 : 3) * (size_t)N * N * N * 16;
+  const size_t smem = sizeof(T) * (GXS ? 4 : 3) * (size_t)N * N * N * 16;
   static bool attr = false;
   if (!attr) {
-    INVDFT_CUDA(cudaFuncSetAttribute(hx_cell_sf_kernel<N, MINB, GXS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_cell_sf_kernel<N, MINB, GXS, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
     attr = true;
   }
@@ -1786,7 +1793,7 @@ static void hx_sf_n(const FeView &fe, const SfMats &mt, const double *vj, const 
   while (C < B && C < 16) C <<= 1;
   const int G = 16 / C;
   const dim3 grid((unsigned)((fe.nc + G - 1) / G), (unsigned)((B + C - 1) / C));
-  hx_cell_sf_kernel<N, MINB, GXS><<<grid, threads, smem, s>>>(fe, mt, vj, x, Ycell, B, C, mode);
+  hx_cell_sf_kernel<N, MINB, GXS, T><<<grid, threads, smem, s>>>(fe, mt, vj, x, Ycell, B, C, mode);
   INVDFT_LAUNCH_CHECK();
 }
 
@@ -1805,8 +1812,7 @@ static void hx_sf_dispatch(const FeView &fe, const SfMats &mt, const double *vj,
   }
 }
 
-void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell,
-                       int B, int gather_mode, int tune, cudaStream_t s) {
+static void launch_group_gather(const FeView &fe, const double *x, int B, int gather_mode, cudaStream_t s) {
   if (gather_mode != GATHER_PLAIN && fe.ngroup > 0) {
     // staging capacity: the largest group's need, at most fe.g_stage doubles
     const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnm, 1) * (B + fe.g_maxnr), fe.g_stage);
@@ -1818,6 +1824,26 @@ void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, con
     group_gather_kernel<<<fe.ngroup, NT, sizeof(double) * (size_t)cap, s>>>(fe, x, B, cap);
     INVDFT_LAUNCH_CHECK();
   }
+}
+
+void launch_hx_cell_sf_f32(const FeView &fe, const SfMatsT<float> &mt, const double *vj, const double *x,
+                           double *Ycell, int B, int gather_mode, cudaStream_t s) {
+  launch_group_gather(fe, x, B, gather_mode, s);
+  switch (fe.n1) {
+    case 2: hx_sf_n<2, 2, false, float>(fe, mt, vj, x, Ycell, B, gather_mode, s); break;
+    case 3: hx_sf_n<3, 2, false, float>(fe, mt, vj, x, Ycell, B, gather_mode, s); break;
+    case 4: hx_sf_n<4, 2, false, float>(fe, mt, vj, x, Ycell, B, gather_mode, s); break;
+    case 5: hx_sf_n<5, 2, false, float>(fe, mt, vj, x, Ycell, B, gather_mode, s); break;
+    case 6: hx_sf_n<6, 2, false, float>(fe, mt, vj, x, Ycell, B, gather_mode, s); break;
+    case 7: hx_sf_n<7, 1, false, float>(fe, mt, vj, x, Ycell, B, gather_mode, s); break;
+    case 8: hx_sf_n<8, 1, false, float>(fe, mt, vj, x, Ycell, B, gather_mode, s); break;
+    default: throw StatusError(5, "matrix-free HX supports FE orders 1..7");
+  }
+}
+
+void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell,
+                       int B, int gather_mode, int tune, cudaStream_t s) {
+  launch_group_gather(fe, x, B, gather_mode, s);
   if (tune == 2 && fe.n1 == 6) {   // two CTAs per SM, derivative lines in shared memory
     hx_sf_n<6, 2, true>(fe, mt, vj, x, Ycell, B, gather_mode, s);
     return;

@@ -78,24 +78,41 @@ void launch_narrow(const double *src, float *dst, int64_t n, cudaStream_t s);
 // w = 1D Gauss weights on [0, 1].
 constexpr int kSfMaxN = 8;
 constexpr int kSfMaxH = kSfMaxN / 2;
-struct SfMats {
-  double phi[kSfMaxN * kSfMaxN];
-  double dq[kSfMaxN * kSfMaxN];
-  double w[kSfMaxN];
+template <typename T> struct SfMatsT {
+  T phi[kSfMaxN * kSfMaxN];
+  T dq[kSfMaxN * kSfMaxN];
+  T w[kSfMaxN];
   // even n1: even-odd halves [q*h + a] (h = n1/2) of the four 1D operators,
   // applied as out[q] = E + O, out[n1-1-q] = E - O (Phi, Phi^T: centro-
   // symmetric) or O - E (Dq, Dq^T: centro-antisymmetric), with
   // E = sum_a Xe[q][a] (in[a] + in[n1-1-a]), O = sum_a Xo[q][a] (in[a] - in[n1-1-a])
-  double phe[kSfMaxH * kSfMaxH], pho[kSfMaxH * kSfMaxH];   // Phi
-  double dqe[kSfMaxH * kSfMaxH], dqo[kSfMaxH * kSfMaxH];   // Dq
-  double pte[kSfMaxH * kSfMaxH], pto[kSfMaxH * kSfMaxH];   // Phi^T
-  double dte[kSfMaxH * kSfMaxH], dto[kSfMaxH * kSfMaxH];   // Dq^T
+  T phe[kSfMaxH * kSfMaxH], pho[kSfMaxH * kSfMaxH];   // Phi
+  T dqe[kSfMaxH * kSfMaxH], dqo[kSfMaxH * kSfMaxH];   // Dq
+  T pte[kSfMaxH * kSfMaxH], pto[kSfMaxH * kSfMaxH];   // Phi^T
+  T dte[kSfMaxH * kSfMaxH], dto[kSfMaxH * kSfMaxH];   // Dq^T
+
+  // the same matrices rounded to another type
+  template <typename U> SfMatsT<U> as() const {
+    SfMatsT<U> o;
+    for (int i = 0; i < kSfMaxN * kSfMaxN; ++i) { o.phi[i] = U(phi[i]); o.dq[i] = U(dq[i]); }
+    for (int i = 0; i < kSfMaxN; ++i) o.w[i] = U(w[i]);
+    for (int i = 0; i < kSfMaxH * kSfMaxH; ++i) {
+      o.phe[i] = U(phe[i]); o.pho[i] = U(pho[i]); o.dqe[i] = U(dqe[i]); o.dqo[i] = U(dqo[i]);
+      o.pte[i] = U(pte[i]); o.pto[i] = U(pto[i]); o.dte[i] = U(dte[i]); o.dto[i] = U(dto[i]);
+    }
+    return o;
+  }
 };
+using SfMats = SfMatsT<double>;
 // matrix-free variant: vj [nc][nq] = v_KS * JxW at the parent quadrature points;
 // tune 0: one CTA per SM allowed the registers it wants, 1: two CTAs per SM,
 // 2: two CTAs per SM with the derivative lines held in shared memory (order 5)
 void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell,
                        int B, int gather_mode, int tune, cudaStream_t s);
+// the same with FP32 arithmetic (FP64 block in, FP64 cell results out): the
+// low rungs of the mixed-precision Chebyshev ladder
+void launch_hx_cell_sf_f32(const FeView &fe, const SfMatsT<float> &mt, const double *vj, const double *x,
+                           double *Ycell, int B, int gather_mode, cudaStream_t s);
 // out[i] = a[i] * b[i]
 void launch_mul(const double *a, const double *b, double *out, int64_t n, cudaStream_t s);
 // bulk-asynchronous staged variant (persistent CTAs, shared-memory panel ring)

@@ -247,10 +247,13 @@ def test_minres_iteration_cap_returns_finite():
     assert np.all(np.isfinite(f)) and st["minres_iters_max"] <= 1
 
 
+@pytest.mark.parametrize("variant", ["sf", "dmma"])
 @pytest.mark.parametrize("name", ["small_lih"])
-def test_mixed_precision_ladder_reaches_fp64_accuracy(name):
-    """MIXED: filter passes on FP32-stored cell matrices, then FP64 passes; the
-    converged result must match the FP64 oracle (eigenvalues 1e-9 Ha, force 1e-6)."""
+def test_mixed_precision_ladder_reaches_fp64_accuracy(name, variant, monkeypatch):
+    """MIXED: early filter passes in FP32 (the FP32 matrix-free kernel, or
+    FP32-stored cell matrices), then FP64 passes; the converged result must
+    match the FP64 oracle (eigenvalues 1e-9 Ha, force 1e-6)."""
+    monkeypatch.setenv("INVDFT_HX_KERNEL", variant)
     P, fn, orc = _pair(name, precision=1, mixed_residual_floor=1e-4)
     pot = P.vxc_init.copy()
     f_g, L_g, st = fn.get_force_vector(pot.copy())

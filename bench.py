@@ -144,6 +144,16 @@ def build_workload(name: str, rank: int):
     return P, dict(t_mesh_s=round(t_mesh, 1), t_setup_s=round(time.time() - t0, 1))
 
 
+_MOLECULE = {"c0_lih": "LiH", "c1_c2h4": "C2H4", "c2_c2h4": "C2H4", "c3_h2o": "H2O", "c4_c8h18": "C8H18"}
+
+
+def workload_name(config: str, P, precision: str) -> str:
+    """The workload both arms name in their JSON line."""
+    mol = _MOLECULE.get(config, config)
+    return (f"{config}: {mol}-like, FE order {P.p}, {P.n_nodes} DoF, {P.n_cells} cells, {P.n_states} states, "
+            f"{P.n_child_cells} v_xc cells / {P.n_child_nodes} nodes, precision {precision}")
+
+
 def hx_probe(args, dev):
     """``--steps`` Lowdin HX applications of a seeded [n_nodes, width] block on
     the workload's mesh at v_xc = the initial guess: the launch sequence the
@@ -273,8 +283,8 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
-                "config": {"workload": f"{args.config} (p={P.p}, {P.n_nodes} DoF, {P.n_cells} cells, "
-                                       f"{P.n_states} states, {P.n_child_nodes} v_xc nodes)"},
+                "config": {"workload": workload_name(args.config, P, args.precision),
+                           "step": "one getForceVector at a new v_xc on the path guess -> v_xc*"},
                 "cpu_baseline": dict(value=v, unit="force-evals/s", **meta),
                 "e2e": {"value": v, "unit": "force-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -373,9 +383,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 (FP32-stored cell matrices in the filter)",
             "data": "synthetic (seeded; see invdft_b200/problem/system.py)",
             "config": {
-                "workload": f"{args.config}: C2H4-like, FE order {P.p}, {P.n_nodes} DoF, {P.n_cells} cells, "
-                            f"{P.n_states} states, {P.n_child_cells} v_xc cells / {P.n_child_nodes} nodes, "
-                            f"precision {args.precision}",
+                "workload": workload_name(args.config, P, args.precision),
                 "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (state block + cell results "
                 f"{(P.n_nodes + P.n_cells * P.nd) * P.n_states * 8 / 1e9:.2f} GB per HX)",
                 "step": "one getForceVector at a new v_xc on the path guess -> v_xc*",

@@ -81,3 +81,21 @@ def test_replica_timing_is_max_over_ranks_gloo():
         assert tmax == pytest.approx(200.0)
         assert v == pytest.approx(4 * 2 / 0.2)
         assert e2e == pytest.approx(4 * 2 / 0.22)
+
+
+def test_bench_workload_names_and_profile_traffic():
+    """Both bench arms name the workload with the same helper, and the captured
+    cell-product traffic of the profiles has the width it was captured at."""
+    import importlib.util
+    import os
+    from types import SimpleNamespace
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(root, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    P = SimpleNamespace(p=5, n_nodes=10, n_cells=2, n_states=16, n_child_cells=3, n_child_nodes=4)
+    name = bench.workload_name("c1_c2h4", P, "fp64")
+    assert name.startswith("c1_c2h4: C2H4-like, FE order 5, 10 DoF")
+    assert bench.workload_name("c0_lih", P, "fp64").startswith("c0_lih: LiH-like")
+    cap = bench._traffic_from_profiles("c1_c2h4:sf:fp64")
+    assert cap["columns"] == 16 and cap["bytes"] > 0

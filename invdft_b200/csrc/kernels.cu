@@ -1637,13 +1637,6 @@ __global__ void force_project_kernel(ChildView cv, const double *__restrict__ S,
 
 std::atomic<long long> g_launches{0};
 
-int pick_blocks(int64_t rows, int64_t min_rows) {
-  int64_t nb = (rows + min_rows - 1) / min_rows;
-  if (nb > 148 * 8) nb = 148 * 8;
-  if (nb < 1) nb = 1;
-  return (int)nb;
-}
-
 }  // namespace
 
 long long launch_count() { return g_launches.load(); }

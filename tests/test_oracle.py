@@ -159,11 +159,13 @@ def test_fermi_level_fills_electrons():
     assert -0.3 < mu < -0.1
 
 
-def test_golden_fixture():
-    """The oracle reproduces its committed output on tiny_h2 (tests/golden/make_golden.py)."""
+@pytest.mark.parametrize("name", ["tiny_h2", "small_lih"])
+def test_golden_fixture(name):
+    """The oracle reproduces its committed output (tests/golden/make_golden.py):
+    tiny_h2, and small_lih with hanging nodes on its refined mesh."""
     from oracle import ForceParams, InverseDFTSolverFunction
-    g = np.load(os.path.join(GOLDEN, "tiny_h2_force.npz"), allow_pickle=True)
-    P = problem("tiny_h2")
+    g = np.load(os.path.join(GOLDEN, f"{name}_force.npz"), allow_pickle=True)
+    P = problem(name)
     fn = InverseDFTSolverFunction(P, ForceParams(**{k: g["params"][()][k] for k in g["params"][()]}))
     f, L, st = fn.get_force_vector(g["pot"].copy())
     assert np.max(np.abs(st.eigenvalues - g["eigenvalues"])) < 1e-10

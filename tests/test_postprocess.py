@@ -75,3 +75,21 @@ def test_locate_rejects_outside_points():
     hi = (P.cell_lo + P.cell_h[:, None]).max(axis=0)
     with pytest.raises(ValueError):
         locate_points(P, hi[None, :] + 1.0)
+
+
+def test_postprocess_golden_fixture():
+    """The oracle's projection and point values reproduce their committed
+    output (tests/golden/make_golden.py), including the reference's point order."""
+    import os
+    from invdft_b200.postprocess import grid_points, locate_points
+    from oracle.postprocess import evaluate, project_vxc_to_parent
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "small_lih_postprocess.npz"))
+    P = problem("small_lih")
+    u = project_vxc_to_parent(P, g["vxc"], float(g["factor_lda"]))
+    assert np.max(np.abs(u - g["parent_nodal"])) < 1e-12 * np.max(np.abs(g["parent_nodal"]))
+    lo = P.cell_lo.min(axis=0)
+    hi = (P.cell_lo + P.cell_h[:, None]).max(axis=0)
+    pts = grid_points(lo + 0.25, hi - 0.25, (9, 7, 5))
+    assert np.array_equal(pts, g["points"])
+    cells, xi = locate_points(P, pts)
+    assert np.max(np.abs(evaluate(P, u, cells, xi) - g["values"])) < 1e-12 * np.max(np.abs(g["values"]))

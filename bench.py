@@ -164,20 +164,21 @@ def hx_probe(args, dev):
     P = build_problem(args.config, target_solver="atoms")
     fn = InverseDFTSolverFunction(P, force_params("fp64"))
     fn.set_potential(P.vxc_init.copy())
-    g = torch.Generator(device=dev).manual_seed(1)
-    x = torch.randn(P.n_nodes, args.hx_width, dtype=torch.float64, device=dev, generator=g)
-    for _ in range(max(args.warmup, 1)):   # first use of a width also autotunes the launch shape
-        fn.hx(x)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        y = fn.hx(x)
-    e1.record()
-    torch.cuda.synchronize()
-    print(json.dumps({"probe": "hx", "workload": args.config, "n_dofs": P.n_nodes, "n_cells": P.n_cells,
-                      "width": args.hx_width, "warmup": max(args.warmup, 1), "applications": args.steps,
-                      "ms_per_hx": e0.elapsed_time(e1) / max(args.steps, 1), "norm": float(y.norm())}))
+    for width in [int(w) for w in str(args.hx_width).split(",")]:
+        g = torch.Generator(device=dev).manual_seed(1)
+        x = torch.randn(P.n_nodes, width, dtype=torch.float64, device=dev, generator=g)
+        for _ in range(max(args.warmup, 1)):   # first use of a width also autotunes the launch shape
+            fn.hx(x)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            y = fn.hx(x)
+        e1.record()
+        torch.cuda.synchronize()
+        print(json.dumps({"probe": "hx", "workload": args.config, "n_dofs": P.n_nodes, "n_cells": P.n_cells,
+                          "width": width, "warmup": max(args.warmup, 1), "applications": args.steps,
+                          "ms_per_hx": e0.elapsed_time(e1) / max(args.steps, 1), "norm": float(y.norm())}))
     fn.close()
 
 
@@ -240,7 +241,7 @@ def main():
                     help="do not time the FP64 path on the same trajectory")
     ap.add_argument("--cpu-sample-cells", type=int, default=400)
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample (profiling runs)")
-    ap.add_argument("--hx-width", type=int, default=0,
+    ap.add_argument("--hx-width", type=str, default="0",
                     help="kernel probe for profiling: --steps Lowdin HX applications of a seeded block of this "
                          "width at v_xc = the initial guess, timed with CUDA events (no force evaluation)")
     args = ap.parse_args()
@@ -259,7 +260,7 @@ def main():
     torch.cuda.set_device(dev)
     threads = os.cpu_count() or 1
 
-    if args.hx_width > 0:
+    if args.hx_width != "0":
         hx_probe(args, dev)
         return
 
@@ -326,7 +327,9 @@ def main():
     gemm_bytes = sum(s["cell_gemm_bytes"] for s in stats)
     gemm_flops = sum(s["cell_gemm_flops"] for s in stats)
     peaks, pk = _peaks()
-    matrix_free = os.environ.get("INVDFT_HX_KERNEL", "sf") == "sf" and P.p <= 7 and args.precision == "fp64"
+    # the matrix-free kernel runs in both precisions (its FP32 instance serves
+    # the low rungs of the mixed ladder); stored cell matrices only on request
+    matrix_free = os.environ.get("INVDFT_HX_KERNEL", "sf") == "sf" and P.p <= 7
     hbm_achieved = gemm_bytes / (gemm_ms / 1000.0) / 1e9 if gemm_ms > 0 else None
     # captured traffic of one launch of a given width, scaled to the mean width
     # of this run's launches (traffic grows with the columns processed)
@@ -380,7 +383,10 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "force-evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64 (FP32-stored cell matrices in the filter)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else ("f64 + f32 (FP32 matrix-free cell products in the early "
+                                                          "Chebyshev passes)" if matrix_free else
+                                                          "f64 + f32 (FP32-stored cell matrices in the early "
+                                                          "Chebyshev passes)"),
             "data": "synthetic (seeded; see invdft_b200/problem/system.py)",
             "config": {
                 "workload": workload_name(args.config, P, args.precision),

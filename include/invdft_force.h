@@ -143,6 +143,8 @@ typedef struct {
   double device_bytes;       /* device memory held by the library after the evaluation */
   double device_bytes_peak;  /* its high-water mark */
   int32_t passes_low;        /* Chebyshev passes filtered with FP32-stored cell matrices */
+  int64_t generation;        /* state generation of the forward half this evaluation ran (see
+                                invdft_force_backward_at) */
 } invdft_force_stats;
 
 /* Defaults of the reference's parameters. */
@@ -176,6 +178,11 @@ invdft_status invdft_force_eval(invdft_ctx *ctx, double *pot, double *force,
 /* InverseDFTSolverFunction::dotProduct with blockSize 1 (:1693-1705). */
 invdft_status invdft_dot(invdft_ctx *ctx, const double *a, const double *b,
                          int64_t n, double *out);
+/* InverseDFTSolverFunction::dotProduct (:1693-1705) with any blockSize:
+ * out[j] = sum over i with i % block_size == j of a[i] b[i], accumulated in
+ * entry order, out [block_size].  Host arrays. */
+invdft_status invdft_dot_blocks(invdft_ctx *ctx, const double *a, const double *b,
+                                int64_t n, int32_t block_size, double *out);
 
 /* Results of the last evaluation (host copies). */
 invdft_status invdft_get_eigen(invdft_ctx *ctx, double *eig, double *occ, double *fermi);
@@ -191,13 +198,22 @@ invdft_status invdft_solve_eigen(invdft_ctx *ctx, double *pot, invdft_force_stat
 /* Backward half of getForceVector for the last invdft_solve_eigen: the block
  * adjoint solves and the projection (:914-1246) giving force = dL/dv_xc
  * [n_child_nodes].  invdft_solve_eigen + invdft_force_backward ==
- * invdft_force_eval. */
+ * invdft_force_eval.  NOT_READY when no forward half ran, or when
+ * invdft_set_potential changed the Hamiltonian since. */
 invdft_status invdft_force_backward(invdft_ctx *ctx, double *force, invdft_force_stats *stats);
+/* The same for the forward half whose stats->generation was `generation`:
+ * NOT_READY when any later forward half (invdft_solve_eigen, invdft_force_eval,
+ * invdft_bfgs_solve) or invdft_set_potential has changed the state since, so a
+ * caller that keeps several forward results (an autograd tape) never receives
+ * dL/dv_xc at another v_xc. */
+invdft_status invdft_force_backward_at(invdft_ctx *ctx, int64_t generation, double *force,
+                                       invdft_force_stats *stats);
 
 /* --- building blocks, exposed for the adjoint interface and for tests --- */
 
 /* v_KS = v_base + v_xc(child -> parent quad) + factor_lda v_lda and the cell
- * Hamiltonians (setVEff + computeCellHamiltonianMatrix, :1367-1388). */
+ * Hamiltonians (setVEff + computeCellHamiltonianMatrix, :1367-1388).  Ends the
+ * validity of the last forward half for invdft_force_backward. */
 invdft_status invdft_set_potential(invdft_ctx *ctx, const double *pot);
 
 /* POST_PROCESS projection of v_xc to the parent mesh (InverseDFTEngine::
@@ -260,8 +276,13 @@ invdft_status invdft_bfgs_solve(invdft_ctx *ctx, double *pot, int32_t max_iter, 
  * L-BFGS or Krylov driver whose vectors live in its own device pool).  Needs no
  * context.  Scratch is a static device array of 296 x 64 doubles held by every
  * GPU that loads the library, so B must be in [1, 64] (BAD_ARG otherwise, with
- * the reason in invdft_last_error(NULL)).  The first call on a device looks up
- * the array's device address and should come before any stream capture.
+ * the reason in invdft_last_error(NULL)).  The library's device code is loaded
+ * lazily: the first call on a device loads the module, which reserves the
+ * array and the kernels' own device memory, so a caller that owns its device
+ * pool makes one warm-up call on each device before handing the device to its
+ * pool or starting a stream capture; later calls allocate nothing.  Every call
+ * looks up the array's device address with the device current (no allocation
+ * once the module is loaded), so the address stays right after a device reset.
  * Calls share the array: calls that overlap on the GPU race.  Asynchronous
  * with respect to the host; d_out [B] is device memory. */
 invdft_status invdft_coldot_noalloc(const double *d_a, const double *d_b, int64_t n, int32_t B,

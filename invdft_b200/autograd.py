@@ -29,7 +29,7 @@ class InverseKSLoss(torch.autograd.Function):
         st = Stats()
         _check(fn.lib, fn.ctx, fn.lib.invdft_solve_eigen(fn.ctx, ptr(pot), C.byref(st)))
         ctx.fn = fn
-        ctx.token = fn._forward_token = object()
+        ctx.generation = int(st.generation)
         ctx.device, ctx.dtype = vxc.device, vxc.dtype
         fn.last_stats = st.as_dict()
         return torch.tensor(st.loss, dtype=torch.float64, device=vxc.device)
@@ -37,11 +37,11 @@ class InverseKSLoss(torch.autograd.Function):
     @staticmethod
     def backward(ctx, grad_L):
         fn = ctx.fn
-        if getattr(fn, "_forward_token", None) is not ctx.token:
-            raise RuntimeError("the solver function ran another forward evaluation before this backward")
         force = np.zeros(fn.n_child)
         st = Stats()
-        _check(fn.lib, fn.ctx, fn.lib.invdft_force_backward(fn.ctx, ptr(force), C.byref(st)))
+        # the library refuses (NOT_READY) if any forward evaluation or potential
+        # change ran on this context after this forward
+        _check(fn.lib, fn.ctx, fn.lib.invdft_force_backward_at(fn.ctx, ctx.generation, ptr(force), C.byref(st)))
         fn.last_backward_stats = st.as_dict()
         g = torch.from_numpy(force).to(device=ctx.device, dtype=ctx.dtype)
         return grad_L * g, None

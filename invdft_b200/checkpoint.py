@@ -2,11 +2,13 @@
 
 Writer: one row per child (Q1) node, ``iNode x y z v`` (writeVxcDataToFile ->
 writeChildMeshDataToFile, InverseDFTSolverFunction.cpp:596-655; one spin).
-Readers: ``read_vxc`` takes rows in node order and checks each row's
-coordinates against the node within ``tol`` (readVxcDataFromFile,
-InverseDFTEngine.cpp:2915-2980); ``search=True`` matches rows to nodes by
-coordinates instead (readVxcDataFromFileWithSearch, :2984-3143).  A mismatch
-raises ValueError where the reference aborts.
+Readers: ``read_vxc`` takes row i as node i, checks the row's coordinates
+against node i within ``tol`` and stores its value at node i, whatever its
+``iNode`` column says (readVxcDataFromFile, InverseDFTEngine.cpp:2915-2980,
+places by row position and uses the column only for its MPI ownership test;
+here a column outside [0, n) is rejected); ``search=True`` matches rows to
+nodes by coordinates instead (readVxcDataFromFileWithSearch, :2984-3143).  A
+mismatch raises ValueError where the reference aborts.
 """
 from __future__ import annotations
 
@@ -38,12 +40,12 @@ def read_vxc(path: str | os.PathLike, node_xyz: np.ndarray, tol: float = 1e-3,
         ids = rows[:, 0].astype(np.int64)
         if np.any(ids < 0) or np.any(ids >= node_xyz.shape[0]):
             raise ValueError("node index out of range")
-        dist = np.linalg.norm(rows[:, 1:4] - node_xyz[ids], axis=1)
+        dist = np.linalg.norm(rows[:, 1:4] - node_xyz, axis=1)
         bad = np.nonzero(dist > tol)[0]
         if bad.size:
             raise ValueError(f"v_xc nodal coordinates differ from the mesh at row {int(bad[0])} "
                              f"(distance {dist[bad[0]]:.3e} > {tol})")
-        out[ids] = rows[:, 4]
+        out[:] = rows[:, 4]
         return out
     from scipy.spatial import cKDTree
     dist, ids = cKDTree(node_xyz).query(data[:, 1:4])

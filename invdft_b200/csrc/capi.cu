@@ -126,11 +126,17 @@ invdft_status invdft_force_eval(invdft_ctx *ctx, double *pot, double *force, dou
 }
 
 invdft_status invdft_dot(invdft_ctx *ctx, const double *a, const double *b, int64_t n, double *out) {
+  return invdft_dot_blocks(ctx, a, b, n, 1, out);
+}
+
+invdft_status invdft_dot_blocks(invdft_ctx *ctx, const double *a, const double *b, int64_t n, int32_t block_size,
+                                double *out) {
   return guard(ctx, [&](invdft::Context &) {
-    if (!a || !b || !out || n < 0) throw invdft::StatusError(INVDFT_BAD_ARG, "bad dot arguments");
-    double s = 0.0;
-    for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
-    *out = s;
+    if (!a || !b || !out || n < 0 || block_size < 1)
+      throw invdft::StatusError(INVDFT_BAD_ARG, "bad dot arguments (null array, n < 0 or block_size < 1)");
+    // entry i accumulates into out[i % block_size], in entry order
+    for (int32_t j = 0; j < block_size; ++j) out[j] = 0.0;
+    for (int64_t i = 0; i < n; ++i) out[i % block_size] += a[i] * b[i];
   });
 }
 
@@ -183,9 +189,20 @@ invdft_status invdft_force_backward(invdft_ctx *ctx, double *force, invdft_force
   });
 }
 
+invdft_status invdft_force_backward_at(invdft_ctx *ctx, int64_t generation, double *force,
+                                       invdft_force_stats *stats) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!force || generation < 0) throw invdft::StatusError(INVDFT_BAD_ARG, "null force or negative generation");
+    invdft_force_stats local{};
+    invdft_force_stats *st = stats ? stats : &local;
+    c.backward(force, st, generation);
+  });
+}
+
 invdft_status invdft_set_potential(invdft_ctx *ctx, const double *pot) {
   return guard(ctx, [&](invdft::Context &c) {
     if (!pot) throw invdft::StatusError(INVDFT_BAD_ARG, "null potential");
+    c.invalidate_forward();   // the backward half would run with this Hamiltonian
     c.pot_d.upload(pot, c.ncn, c.stream);
     c.set_potential_device(c.pot_d.p);
     INVDFT_CUDA(cudaStreamSynchronize(c.stream));

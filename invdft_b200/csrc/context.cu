@@ -1320,6 +1320,7 @@ struct StageTimer {
 // (InverseDFTSolverFunction.cpp:671-912).  The eigenvectors stay in the context
 // (stored once) for the backward half.
 void Context::forward(double *pot, invdft_force_stats *st) {
+  invalidate_forward();   // a forward that fails half way leaves no usable state
   n_hx = 0;
   n_hx_cols = 0;
   fwd_launches0 = launch_count();
@@ -1341,6 +1342,7 @@ void Context::forward(double *pot, invdft_force_stats *st) {
   if (!std::isfinite(sums[0])) throw StatusError(INVDFT_NONFINITE, "non-finite loss");
   last_loss = sums[0];
   have_forward = true;
+  st->generation = generation;
   // zero the constrained entries of the potential on exit (:1295-1298)
   for (int64_t r : cchild.h_rows) pot[r] = 0.0;
   loss_prev = sums[0];
@@ -1353,8 +1355,12 @@ void Context::forward(double *pot, invdft_force_stats *st) {
 // constraints, psi.p at the child quadrature points, projection onto the v_xc
 // nodes (InverseDFTSolverFunction.cpp:914-1246).  Uses the eigenvectors and u
 // of the last forward half; keeps no Krylov vectors afterwards.
-void Context::backward(double *force, invdft_force_stats *st) {
-  if (!have_forward) throw StatusError(INVDFT_NOT_READY, "backward needs a forward evaluation first");
+void Context::backward(double *force, invdft_force_stats *st, int64_t expected_generation) {
+  if (!have_forward)
+    throw StatusError(INVDFT_NOT_READY, "backward needs a forward evaluation first (or the potential changed since)");
+  if (expected_generation >= 0 && expected_generation != generation)
+    throw StatusError(INVDFT_NOT_READY, "the context ran another forward evaluation (or changed its potential) "
+                                        "after the one this backward belongs to");
   S.zero(stream);
   StageTimer t_adj(stream);
   double t_transfer = 0.0;
@@ -1406,6 +1412,7 @@ void Context::backward(double *force, invdft_force_stats *st) {
   st->n_launches = launch_count() - fwd_launches0;
   st->device_bytes = (double)device_bytes().load();
   st->device_bytes_peak = (double)device_bytes_peak().load();
+  st->generation = generation;
   profile_end(st);
   check_device_error();
 }

@@ -145,9 +145,15 @@ class Context {
   void adj_minres(double *d_x, double tol, int maxit, std::vector<int> &iters);
   // full evaluation = forward half + backward half
   void forward(double *pot, invdft_force_stats *st);
-  void backward(double *force, invdft_force_stats *st);
+  // expected_generation < 0: the current forward half, whichever it is
+  void backward(double *force, invdft_force_stats *st, int64_t expected_generation = -1);
   void eval(double *pot, double *force, double *loss, invdft_force_stats *st);
   bool have_forward = false;
+  // Bumped by every forward half and by every call that changes what the
+  // backward half reads (the potential); a backward for an older forward is
+  // refused instead of returning dL/dv_xc at another v_xc.
+  int64_t generation = 0;
+  void invalidate_forward() { have_forward = false; ++generation; }
   double last_loss = 0.0;
   long long fwd_launches0 = 0;
   void accumulate_child_products(const double *d_psi, const double *d_p, int Bw);

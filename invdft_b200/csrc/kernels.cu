@@ -603,8 +603,10 @@ __global__ void __launch_bounds__(NT, 1) hx_gemm_bulk_kernel(FeView fe, const do
     bulk_g2s(stages + (sq % S) * (int64_t)PW * ldh,
              H + e * (int64_t)((nd + 1) >> 1) * 2 * ldh + (int64_t)c0 * ldh, bytes, bar);
   };
+  int64_t n_issued = 0;     // thread 0: panels issued so far
+  int64_t first_open = -1;  // thread 0: first panel its own wait gave up on
   if (tid == 0)
-    for (int64_t sq = 0; sq < min((int64_t)S, total); ++sq) issue(sq);
+    for (int64_t sq = 0; sq < min((int64_t)S, total); ++sq) issue(sq), n_issued = sq + 1;
   bool ok = true;
   const int i = tid;
   for (int64_t t = 0; t < ncell; ++t) {
@@ -642,6 +644,7 @@ __global__ void __launch_bounds__(NT, 1) hx_gemm_bulk_kernel(FeView fe, const do
           if (++it > kWaitLimit) {
             ok = false;
             atomicExch(fe.err, 1);
+            if (tid == 0) first_open = sq;
             break;
           }
         }
@@ -668,6 +671,7 @@ __global__ void __launch_bounds__(NT, 1) hx_gemm_bulk_kernel(FeView fe, const do
       if (tid == 0 && ok && sq + S < total) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         issue(sq + S);
+        n_issued = sq + S + 1;
       }
     }
     if (ok && i < nd) {
@@ -677,6 +681,18 @@ __global__ void __launch_bounds__(NT, 1) hx_gemm_bulk_kernel(FeView fe, const do
 #pragma unroll
         for (int b = 0; b < BC; ++b)
           if (b < B) yo[b] = acc[b];
+      }
+    }
+  }
+  // after a wait gave up, copies issued from there on may still be writing
+  // this CTA's shared memory: thread 0 waits for them (bounded again) before
+  // the CTA retires and its shared memory can be handed to another CTA.  Thread
+  // 0 stops issuing once its own wait fails, so each stage holds at most one
+  // such copy, with the parity of its panel.
+  if (tid == 0 && first_open >= 0) {
+    for (int64_t sq = first_open; sq < n_issued; ++sq) {
+      long long it = 0;
+      while (!mbar_try_wait(&bars[sq % S], (uint32_t)((sq / S) & 1)) && ++it <= kWaitLimit) {
       }
     }
   }

@@ -14,7 +14,15 @@
 // it keeps the last call's contents; each call overwrites every partial it
 // later reads, so nothing needs clearing, but calls that overlap on the GPU
 // (different streams, no ordering between them) race on it.
-#include <mutex>
+//
+// The module is loaded lazily: the first call on a device loads it, which is
+// when the array and the kernels' own device memory are reserved.  A caller
+// that owns its device pool makes one warm-up call per device before it hands
+// the device to the pool or starts a stream capture.  The array's name in host
+// code is a host-side stand-in, not a device address, so every call asks the
+// runtime for the address with the device current; once the module is loaded
+// the lookup allocates nothing, and it stays right when a device reset or a
+// new primary context reloads the module at another address.
 #include <string>
 
 #include "../../include/invdft_force.h"
@@ -30,10 +38,6 @@ constexpr int kNoallocBlocks = 296;  // 2 x 148 SMs
 constexpr int kNoallocMaxCols = 64;
 static __device__ __align__(256) double g_noalloc_partials[kNoallocBlocks * kNoallocMaxCols];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mtx;
-double *g_scratch[kMaxDevices] = {};
-
 }  // namespace
 
 extern "C" invdft_status invdft_coldot_noalloc(const double *d_a, const double *d_b, int64_t n, int32_t B,
@@ -48,27 +52,19 @@ extern "C" invdft_status invdft_coldot_noalloc(const double *d_a, const double *
     return INVDFT_BAD_ARG;
   }
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+  if (cudaGetDevice(&dev) != cudaSuccess) {
     invdft::set_thread_error("invdft_coldot_noalloc: no usable current CUDA device");
     return INVDFT_CUDA_ERROR;
   }
-  double *scratch = nullptr;
-  {
-    // set-up once per device, with that device current: the array's name in
-    // host code is not a device address, so ask the runtime for it
-    std::lock_guard<std::mutex> lock(g_mtx);
-    if (!g_scratch[dev]) {
-      void *p = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
-      if (e != cudaSuccess || !p) {
-        invdft::set_thread_error(std::string("invdft_coldot_noalloc: cudaGetSymbolAddress failed: ") +
-                                 cudaGetErrorString(e));
-        return INVDFT_CUDA_ERROR;
-      }
-      g_scratch[dev] = static_cast<double *>(p);
-    }
-    scratch = g_scratch[dev];
+  // the device address of the array in the current device's context
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+  if (e != cudaSuccess || !p) {
+    invdft::set_thread_error(std::string("invdft_coldot_noalloc: cudaGetSymbolAddress failed on device ") +
+                             std::to_string(dev) + ": " + cudaGetErrorString(e));
+    return INVDFT_CUDA_ERROR;
   }
+  double *scratch = static_cast<double *>(p);
   try {
     invdft::launch_coldot(d_a, d_b, n, B, scratch, kNoallocBlocks, d_out, static_cast<cudaStream_t>(stream));
   } catch (const std::exception &ex) {

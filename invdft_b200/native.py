@@ -25,6 +25,7 @@ EXPORTED = [
     "invdft_adjoint_vmult", "invdft_adjoint_precondition_jacobi",
     "invdft_adjoint_precondition_jacobi_sqrt", "invdft_adjoint_distribute_x", "invdft_adjoint_solve",
     "invdft_bfgs_solve", "invdft_coldot_noalloc", "invdft_project_vxc_to_parent", "invdft_evaluate_parent_field",
+    "invdft_force_backward_at", "invdft_dot_blocks",
 ]
 
 
@@ -80,7 +81,7 @@ class Stats(C.Structure):
         ("n_cell_gemm", C.c_int32), ("ms_cell_gemm", C.c_double), ("cell_gemm_bytes", C.c_double),
         ("cell_gemm_flops", C.c_double), ("n_launches", C.c_int64), ("degree", C.c_int32),
         ("upper_bound", C.c_double), ("device_bytes", C.c_double), ("device_bytes_peak", C.c_double),
-        ("passes_low", C.c_int32),
+        ("passes_low", C.c_int32), ("generation", C.c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -115,6 +116,8 @@ def load() -> C.CDLL:
         "invdft_get_child_quad_products": (C.c_int, [vp, _f64p]),
         "invdft_solve_eigen": (C.c_int, [vp, _f64p, _P(Stats)]),
         "invdft_force_backward": (C.c_int, [vp, _f64p, _P(Stats)]),
+        "invdft_force_backward_at": (C.c_int, [vp, C.c_int64, _f64p, _P(Stats)]),
+        "invdft_dot_blocks": (C.c_int, [vp, _f64p, _f64p, C.c_int64, C.c_int32, _f64p]),
         "invdft_set_potential": (C.c_int, [vp, _f64p]),
         "invdft_hx": (C.c_int, [vp, vp, vp, C.c_int32]),
         "invdft_project_vxc_to_parent": (C.c_int, [vp, _f64p, _f64p]),

@@ -91,14 +91,15 @@ class InverseDFTSolverFunction:
         loss[:] = [L]
 
     def dotProduct(self, a, b, blockSize: int = 1):
-        if blockSize != 1:
-            a = f64(a).reshape(-1, blockSize)
-            b = f64(b).reshape(-1, blockSize)
-            return list(np.einsum("ij,ij->j", a, b))
+        """dotProduct (InverseDFTSolverFunction.cpp:1693-1705): entry i
+        accumulates into out[i % blockSize]."""
         a, b = f64(a), f64(b)
-        out = C.c_double()
-        _check(self.lib, self.ctx, self.lib.invdft_dot(self.ctx, ptr(a), ptr(b), a.size, C.byref(out)))
-        return [out.value]
+        if a.size != b.size:
+            raise ValueError("dotProduct of vectors of different lengths")
+        out = np.zeros(int(blockSize))
+        _check(self.lib, self.ctx, self.lib.invdft_dot_blocks(self.ctx, ptr(a), ptr(b), a.size, int(blockSize),
+                                                               ptr(out)))
+        return list(out)
 
     def dot_product(self, a, b) -> float:
         return self.dotProduct(a, b)[0]

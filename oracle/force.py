@@ -224,6 +224,15 @@ class InverseDFTSolverFunction:
         """dotProduct with blockSize 1 (InverseDFTSolverFunction.cpp:1693-1705)."""
         return float(np.dot(a, b))
 
+    @staticmethod
+    def dot_product_blocks(a, b, block_size: int):
+        """dotProduct (InverseDFTSolverFunction.cpp:1693-1705): entry i adds
+        a_i b_i to out[i % blockSize], in entry order."""
+        out = [0.0] * block_size
+        for i, (x, y) in enumerate(zip(np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64))):
+            out[i % block_size] += float(x) * float(y)
+        return out
+
 
 def initial_subspace(n: int, N: int, free: np.ndarray) -> np.ndarray:
     """Deterministic start block X[i, j] = hash_uniform(i * N + j, salt 11), free rows."""

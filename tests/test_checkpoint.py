@@ -35,3 +35,22 @@ def test_coordinate_mismatch_is_an_error(tmp_path):
     write_vxc(f, P.child_node_xyz + 0.01, np.zeros(P.n_child_nodes))
     with pytest.raises(ValueError):
         read_vxc(f, P.child_node_xyz)
+
+
+def test_ordered_reader_places_by_row_position(tmp_path):
+    """readVxcDataFromFile (InverseDFTEngine.cpp:2935-2975) checks row i against
+    node i and stores row i at node i; a duplicated iNode column does not move
+    values, and a column outside [0, n) is rejected."""
+    from invdft_b200.checkpoint import read_vxc
+    P = problem("tiny_h2")
+    n = P.n_child_nodes
+    v = np.random.default_rng(4).standard_normal(n)
+    ids = np.arange(n)
+    ids[1] = 0                                   # duplicated id
+    f = tmp_path / "vxc_dup"
+    np.savetxt(f, np.column_stack([ids, P.child_node_xyz, v]))
+    assert np.array_equal(read_vxc(f, P.child_node_xyz), np.loadtxt(f)[:, 4])
+    ids[2] = n + 5
+    np.savetxt(f, np.column_stack([ids, P.child_node_xyz, v]))
+    with pytest.raises(ValueError):
+        read_vxc(f, P.child_node_xyz)

@@ -85,3 +85,26 @@ def test_backward_refuses_a_stale_forward():
     inverse_ks_loss(torch.tensor(P.vxc_init * 1.01), fn)   # another forward on the same context
     with pytest.raises(RuntimeError):
         L1.backward()
+
+
+def test_library_refuses_backward_after_state_changes():
+    """The C ABI itself refuses (NOT_READY) a backward whose forward is no
+    longer the context's state: after a getForceVector at another v_xc, and
+    after set_potential, whichever Python object holds the forward."""
+    import ctypes as C
+    from invdft_b200.native import Stats, ptr
+    P = problem("tiny_h2")
+    fn = _fn(P)
+    lib = fn.lib
+    st = Stats()
+    pot = P.vxc_init.copy()
+    assert lib.invdft_solve_eigen(fn.ctx, ptr(pot), C.byref(st)) == 0
+    gen = int(st.generation)
+    force = np.zeros(P.n_child_nodes)
+    assert lib.invdft_force_backward_at(fn.ctx, gen, ptr(force), C.byref(Stats())) == 0
+    fn.get_force_vector(P.vxc_init * 1.01)                 # a later forward half
+    assert lib.invdft_force_backward_at(fn.ctx, gen, ptr(force), C.byref(Stats())) == 7
+    assert lib.invdft_solve_eigen(fn.ctx, ptr(P.vxc_init.copy()), C.byref(st)) == 0
+    fn.set_potential(P.vxc_init * 0.99)                     # the Hamiltonian changed
+    assert lib.invdft_force_backward(fn.ctx, ptr(force), C.byref(Stats())) == 7
+    assert lib.invdft_force_backward_at(fn.ctx, int(st.generation), ptr(force), C.byref(Stats())) == 7

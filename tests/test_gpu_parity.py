@@ -294,3 +294,14 @@ def test_sf_launch_shapes_are_bitwise_identical(name, monkeypatch):
     for shape in shapes[1:] + ["auto"]:
         for B in (1, 5, 16):
             assert np.array_equal(out[(shape, B)], out[("0", B)]), (shape, B)
+
+
+def test_dot_product_blocks_matches_oracle():
+    """dotProduct with blockSize 1 and 3 (InverseDFTSolverFunction.cpp:1693-1705),
+    summed in entry order: bit-identical to the oracle's loop."""
+    from oracle import InverseDFTSolverFunction as Oracle
+    P, fn, _ = _pair("tiny_h2")
+    rng = np.random.default_rng(21)
+    a, b = rng.standard_normal(3001), rng.standard_normal(3001)
+    for bs in (1, 3):
+        assert fn.dotProduct(a, b, bs) == Oracle.dot_product_blocks(a, b, bs)

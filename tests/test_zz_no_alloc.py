@@ -4,8 +4,9 @@ invdft_coldot_noalloc is for callers that must not let the library allocate
 device memory while they run (their vectors live in their own device pool, as
 in an outer L-BFGS or Krylov driver).  It keeps its scratch in a static device
 array; this test calls it twice in a row through the C ABI and checks both
-results against invdft_dot, and checks that a block wider than its scratch is
-rejected.  It sits in its own file, collected last.
+results against the library's existing dot product (invdft_dot) and against
+numpy, and checks that a block wider than its scratch is rejected.  It sits in
+its own file, collected last.
 """
 import ctypes as C
 
@@ -45,6 +46,7 @@ def test_noalloc_coldot_matches_dot_twice():
         for j in range(B):
             ref = fn.dot_product(np.ascontiguousarray(a[:, j]), np.ascontiguousarray(b[:, j]))
             assert abs(got[j] - ref) <= 1e-12 * max(1.0, abs(ref)) * np.sqrt(n)
+            assert abs(got[j] - float(np.dot(a[:, j], b[:, j]))) <= 1e-12 * max(1.0, abs(ref)) * np.sqrt(n)
 
 
 def test_noalloc_coldot_rejects_wider_than_scratch():

@@ -7,7 +7,11 @@ run visits them.  Default workload: the ethylene-like system of the FP64
 configuration (FE order 5, ~1.3e6 DoF, 16 states), synthetic inputs.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--config c1_c2h4] [--cpu-sample-cells 400]
+                  [--config c1_c2h4] [--precision fp64|mixed] [--ref-budget-s 240]
+
+The reference arm (--impl reference) runs no CUDA: it times whole force
+evaluations of the C++/OpenMP restatement of the path (oracle/cpu) on the
+host cores, on the same workload, trajectory and knobs.
 
 Multi-GPU: the force evaluation does not shard (one GPU per evaluation), so
 N > 1 runs N independent replicas (weak scaling) and reports their summed
@@ -116,32 +120,31 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def force_knobs(prec: str) -> dict:
+    """Hot-path parameters of the benchmark (both arms)."""
+    return dict(cheb_degree=0, cheby_tol=1e-6, initial_tol_cheb=1e-6, adjoint_initial_tol=1e-8,
+                adjoint_max_iter=5000, max_cheb_passes=100, precision=0 if prec == "fp64" else 1)
+
+
 def force_params(prec: str):
     from invdft_b200 import native
-    return native.default_params(cheb_degree=0, cheby_tol=1e-6, initial_tol_cheb=1e-6,
-                                 adjoint_initial_tol=1e-8, adjoint_max_iter=5000, max_cheb_passes=100,
-                                 precision=0 if prec == "fp64" else 1)
+    return native.default_params(**force_knobs(prec))
 
 
-def build_workload(name: str, rank: int):
-    """Problem with rho* from an FP64 forward solve on the GPU at v_xc*."""
-    from invdft_b200.problem.system import build_problem, set_target_density
-    from invdft_b200.solver import InverseDFTSolverFunction
-    from invdft_b200 import native
+TARGET = "superposed neutral-atom Gaussian densities"
+
+
+def build_workload(name: str):
+    """The configuration's mesh, potentials and v_xc mesh, built on the host.
+
+    The target density is the superposition of the atoms' Gaussian clouds, the
+    same in both arms (no forward solve, no GPU): every force evaluation costs
+    the same whatever the target, and a reachable target only matters for
+    runs to convergence (``--converge``)."""
+    from invdft_b200.problem.system import build_problem
     t0 = time.time()
     P = build_problem(name, target_solver="atoms")
-    t_mesh = time.time() - t0
-    fwd = InverseDFTSolverFunction(P, native.default_params(cheb_degree=0, cheby_tol=1e-9,
-                                                            initial_tol_cheb=1e-9, max_cheb_passes=200))
-    fwd.solve_eigen(P.vxc_exact.copy())
-    e, occ, mu = fwd.eigen()
-    psi = fwd.psi()
-    rho_q = fwd.density()
-    rho_n = 2.0 * np.sum(occ[None, :] * psi * psi, axis=1)
-    fwd.close()
-    set_target_density(P, rho_q, rho_n)
-    P.extras["target_eigenvalues"] = e
-    return P, dict(t_mesh_s=round(t_mesh, 1), t_setup_s=round(time.time() - t0, 1))
+    return P, dict(t_setup_s=round(time.time() - t0, 1), target_density=TARGET)
 
 
 _MOLECULE = {"c0_lih": "LiH", "c1_c2h4": "C2H4", "c2_c2h4": "C2H4", "c3_h2o": "H2O", "c4_c8h18": "C8H18"}
@@ -199,34 +202,68 @@ def trajectory(P, k: int, total: int):
     return P.vxc_init + a * (P.vxc_exact - P.vxc_init)
 
 
-def cpu_sample(P, n_hx_columns: int, N: int, cells: int, threads: int):
-    """FP64 oracle HX timed on a bounded sample of cells, scaled to one evaluation."""
-    from oracle.fe import CellOps
-    import copy
-    sub = copy.copy(P)
-    n = min(cells, P.n_cells)
-    # restrict the cell loop of the oracle's HX to the first n cells
-    sub.n_cells = n
-    sub.cell_nodes = P.cell_nodes[:n]
-    sub.cell_h = P.cell_h[:n]
-    sub.jxw = P.jxw[: n * P.nq]
-    ops = CellOps(sub)
-    ops.cell_hamiltonians(P.v_base[: n * P.nq])
-    x = np.random.default_rng(0).standard_normal((P.n_nodes, N))
-    ops.hx(x)
+def cpu_evaluation(P, prec: str, threads: int, k: int, total: int, state=None):
+    """One whole getForceVector of the C++/OpenMP restatement (oracle/cpu) on the
+    host cores at trajectory point k.  ``state`` (psi, eig, counter, loss_prev,
+    tol_cheb, adjoint_tol) hands over the GPU context's state before that
+    point, so the CPU repeats exactly the evaluation the GPU timed."""
+    from oracle.cpu import CpuForce
+    cpu = CpuForce(P, threads=threads, **{**force_knobs("fp64"), "precision": 0})
+    if state is not None:
+        cpu.set_state(**state)
+    pot = trajectory(P, k, total)
     t0 = time.perf_counter()
-    reps = 0
-    while True:
-        ops.hx(x)
-        reps += 1
-        if time.perf_counter() - t0 > 10.0 or reps >= 50:
+    f, L, st = cpu.get_force_vector(pot)
+    dt = time.perf_counter() - t0
+    cpu.close()
+    return f, L, st, dt
+
+
+def run_reference(args, threads: int):
+    """The reference arm: the CPU restatement of the path on the host cores,
+    whole force evaluations on the same workload, trajectory and knobs as the
+    GPU arm.  No CUDA is touched.  One untimed warm-up evaluation stands for
+    the GPU arm's warm-up steps (its counter and tolerances are then set as
+    after ``--warmup`` evaluations); then evaluations are timed one after
+    another until ``--steps`` are done or ``--ref-budget-s`` is spent."""
+    from oracle.cpu import CpuForce
+    P, info = build_workload(args.config)
+    total = args.warmup + args.steps
+    cpu = CpuForce(P, threads=threads, **{**force_knobs("fp64"), "precision": 0})
+    w0 = time.perf_counter()
+    _, Lw, stw = cpu.get_force_vector(trajectory(P, max(args.warmup - 1, 0), total))
+    t_warm = time.perf_counter() - w0
+    cpu.set_state(counter=max(args.warmup, 1), loss_prev=Lw, tol_cheb=stw["cheb_tol"],
+                  adjoint_tol=stw["adjoint_tol"])
+    times, stats = [], []
+    t_begin = time.perf_counter()
+    for k in range(args.warmup, total):
+        t0 = time.perf_counter()
+        _, L, st = cpu.get_force_vector(trajectory(P, k, total))
+        times.append(time.perf_counter() - t0)
+        stats.append(st)
+        if time.perf_counter() - t_begin + times[-1] > args.ref_budget_s:
             break
-    t_hx = (time.perf_counter() - t0) / reps * (P.n_cells / n)
-    t_eval = t_hx * n_hx_columns / N
-    return 1.0 / t_eval, dict(kind="port", cores=threads,
-                              sample=f"oracle FP64 Lowdin HX on {n} of {P.n_cells} cells, {reps} reps of "
-                                     f"B={N}, scaled by cells and by the {n_hx_columns} HX columns one "
-                                     f"evaluation issues (RR, MINRES vector work and transfers not counted)")
+    cpu.close()
+    n = len(times)
+    v = n / sum(times)
+    sample = (f"{n} whole FP64 force evaluations (eigensolve, density, block MINRES, projection) of the C++/OpenMP "
+              f"restatement on {threads} host threads, at trajectory points {args.warmup}..{args.warmup + n - 1} of "
+              f"{total}, after one untimed warm-up evaluation ({t_warm:.1f} s); {n} of the {args.steps} requested "
+              f"steps fit the {args.ref_budget_s:.0f} s budget")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "force-evals/s", "n_gpus": args.gpus,
+            "steps": n, "steps_requested": args.steps, "warmup": 1, "warmup_requested": args.warmup,
+            "ms_per_step": 1000.0 * sum(times) / n, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_name(args.config, P, "fp64"),
+                       "step": "one getForceVector at a new v_xc on the path guess -> v_xc*",
+                       "chebyshev_passes": [s["passes"] for s in stats],
+                       "minres_iters_max": [s["minres_iters_max"] for s in stats],
+                       "hx_columns": [s["n_hx_columns"] for s in stats],
+                       "loss": [s["loss"] for s in stats], "s_per_step": times, **info},
+            "cpu_baseline": dict(value=v, unit="force-evals/s", kind="port", cores=threads, sample=sample),
+            "e2e": {"value": v, "unit": "force-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
 
 
 def main():
@@ -239,8 +276,9 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="do not time the FP64 path on the same trajectory")
-    ap.add_argument("--cpu-sample-cells", type=int, default=400)
-    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample (profiling runs)")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU evaluation (profiling runs)")
+    ap.add_argument("--ref-budget-s", type=float, default=240.0,
+                    help="reference arm: stop timing CPU evaluations once this much time is spent")
     ap.add_argument("--hx-width", type=str, default="0",
                     help="kernel probe for profiling: --steps Lowdin HX applications of a seeded block of this "
                          "width at v_xc = the initial guess, timed with CUDA events (no force evaluation)")
@@ -249,6 +287,14 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        # host cores only: rank 0 runs, the others leave without work
+        if rank == 0:
+            run_reference(args, threads)
+        return
+
     import torch
     dist = None
     if world > 1:
@@ -258,40 +304,12 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    threads = os.cpu_count() or 1
 
     if args.hx_width != "0":
         hx_probe(args, dev)
         return
 
-    if args.impl == "reference":
-        if rank != 0:
-            if dist:
-                dist.destroy_process_group()
-            return
-        P, info = build_workload(args.config, rank)
-        from invdft_b200.solver import InverseDFTSolverFunction
-        fn = InverseDFTSolverFunction(P, force_params(args.precision))
-        fn.get_force_vector(trajectory(P, 0, 1))
-        ncols = fn.last_stats["n_hx_columns"]
-        fn.close()
-        vals = []
-        for _ in range(max(args.steps, 1)):
-            v, meta = cpu_sample(P, ncols, P.n_states, args.cpu_sample_cells, threads)
-            vals.append(v)
-        v = float(np.median(vals))
-        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "force-evals/s", "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic",
-                "config": {"workload": workload_name(args.config, P, args.precision),
-                           "step": "one getForceVector at a new v_xc on the path guess -> v_xc*"},
-                "cpu_baseline": dict(value=v, unit="force-evals/s", **meta),
-                "e2e": {"value": v, "unit": "force-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
-        return
-
-    P, info = build_workload(args.config, rank)
+    P, info = build_workload(args.config)
     from invdft_b200.solver import InverseDFTSolverFunction
     fn = InverseDFTSolverFunction(P, force_params(args.precision))
     lib = fn.lib
@@ -299,13 +317,21 @@ def main():
     total = args.warmup + args.steps
     pinned_pot = torch.empty(P.n_child_nodes, dtype=torch.float64).pin_memory()
     pinned_force = torch.empty(P.n_child_nodes, dtype=torch.float64).pin_memory()
+    last = None
     for k in range(args.warmup):
         pot = trajectory(P, k, total)
-        fn.get_force_vector(pot.copy())
+        last = fn.get_force_vector(pot.copy())
+    # the context's state before the first timed step, for the CPU repeat of it
+    state = None
+    if last is not None and rank == 0 and world == 1 and not args.no_cpu_baseline:
+        e, _, _ = fn.eigen()
+        state = dict(psi=fn.psi(), eig=e, counter=args.warmup, loss_prev=last[1], tol_cheb=last[2]["cheb_tol"],
+                     adjoint_tol=last[2]["adjoint_tol"])
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     stats = []
+    first_force = None
     t_e2e = 0.0
     with ClockSampler(local) as clk:
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -316,6 +342,8 @@ def main():
             pinned_pot.numpy()[:] = trajectory(P, k, total)
             f, L, st = fn.get_force_vector(pinned_pot.numpy())
             pinned_force.numpy()[:] = f
+            if first_force is None:
+                first_force = f.copy()
             stats.append(st)
         torch.cuda.nvtx.range_pop()
         ev1.record()
@@ -333,7 +361,7 @@ def main():
     hbm_achieved = gemm_bytes / (gemm_ms / 1000.0) / 1e9 if gemm_ms > 0 else None
     # captured traffic of one launch of a given width, scaled to the mean width
     # of this run's launches (traffic grows with the columns processed)
-    cap = _traffic_from_profiles(f"{args.config}:{'sf' if matrix_free else 'dmma'}:{args.precision}")
+    cap = _traffic_from_profiles(f"{args.config}:{'sf' if matrix_free else 'dmma'}:fp64")
     mean_cols = sum(s["n_hx_columns"] for s in stats) / max(n_gemm, 1)
     per_launch_traffic = cap["bytes"] * mean_cols / cap["columns"] if isinstance(cap, dict) else cap
     if matrix_free:
@@ -371,15 +399,30 @@ def main():
         torch.cuda.synchronize()
         v64, _, ms64 = aggregate(e0.elapsed_time(e1), 1.0, args.steps, world, dist)
         fp64_cmp = {"value": v64, "ms_per_step": ms64 / args.steps, "passes": [s["passes"] for s in f64_stats],
+                    "minres_iters_max": [s["minres_iters_max"] for s in f64_stats],
+                    "stage_ms_mean": {k: float(np.mean([s[f"ms_{k}"] for s in f64_stats]))
+                                      for k in ("eigen", "density", "adjoint", "transfer")},
                     "speedup_mixed_vs_fp64": value / v64,
                     "max_abs_loss_diff_vs_fp64": max(abs(a["loss"] - b["loss"]) for a, b in zip(stats, f64_stats))}
         fn64.close()
     if rank == 0:
-        if args.no_cpu_baseline:
-            cpu_v, cpu_meta = None, dict(kind="port", cores=threads, sample="skipped (--no-cpu-baseline)")
+        if state is None:
+            cpu_v, cpu_meta = None, dict(kind="port", cores=threads,
+                                         sample="skipped (--no-cpu-baseline, no warm-up, or more than one rank)")
+            cpu_check = None
         else:
-            cpu_v, cpu_meta = cpu_sample(P, int(np.mean([s["n_hx_columns"] for s in stats])), P.n_states,
-                                         args.cpu_sample_cells, threads)
+            f_c, L_c, st_c, dt = cpu_evaluation(P, args.precision, threads, args.warmup, total, state)
+            cpu_v = 1.0 / dt
+            cpu_meta = dict(kind="port", cores=threads,
+                            sample=f"one whole FP64 force evaluation of the C++/OpenMP restatement on {threads} host "
+                                   f"threads, repeating the first timed step (trajectory point {args.warmup}) from "
+                                   f"the GPU context's state before it: {st_c['passes']} Chebyshev passes, MINRES "
+                                   f"max {st_c['minres_iters_max']} iterations, {dt:.1f} s")
+            cpu_check = {"force_rel_l2_vs_gpu": float(np.linalg.norm(f_c - first_force) /
+                                                      max(np.linalg.norm(f_c), 1e-300)),
+                         "loss_cpu": L_c, "loss_gpu": stats[0]["loss"],
+                         "passes_cpu_gpu": [st_c["passes"], stats[0]["passes"]],
+                         "minres_iters_max_cpu_gpu": [st_c["minres_iters_max"], stats[0]["minres_iters_max"]]}
         line = {
             "metric": METRIC, "value": value, "unit": "force-evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -394,7 +437,7 @@ def main():
                 f"{(P.n_nodes + P.n_cells * P.nd) * P.n_states * 8 / 1e9:.2f} GB per HX)",
                 "step": "one getForceVector at a new v_xc on the path guess -> v_xc*",
                 "chebyshev_passes": [s["passes"] for s in stats],
-                "chebyshev_passes_fp32_stored": [s["passes_low"] for s in stats],
+                "chebyshev_passes_low_precision": [s["passes_low"] for s in stats],
                 "fp64_same_trajectory": fp64_cmp,
                 "chebyshev_degree": [s["degree"] for s in stats],
                 "spectrum_upper_bound": stats[-1]["upper_bound"],
@@ -403,6 +446,8 @@ def main():
                 "stage_ms_mean": {k: float(np.mean([s[f"ms_{k}"] for s in stats]))
                                   for k in ("eigen", "density", "adjoint", "transfer")},
                 "hx_kernel": "matrix-free sum factorisation" if matrix_free else "stored cell matrices (DMMA)",
+                "device_bytes_peak": stats[-1]["device_bytes_peak"],
+                "cpu_repeat_of_first_step": cpu_check,
                 "loss": [s["loss"] for s in stats], **info},
             "e2e": {"value": e2e, "unit": "force-evals/s", "h2d_bytes_per_step": 8 * P.n_child_nodes,
                     "d2h_bytes_per_step": 8 * P.n_child_nodes + 8},

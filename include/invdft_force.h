@@ -261,6 +261,28 @@ invdft_status invdft_adjoint_distribute_x(invdft_ctx *ctx, double *d_x);
 invdft_status invdft_adjoint_solve(invdft_ctx *ctx, double *d_x, double tol, int32_t max_iter,
                                    int32_t *iters);
 
+/* Integer index data the library built on the device from the descriptor,
+ * downloaded as int32 for exact comparison with the caller's (the reference's
+ * cell->DoF maps of computeCellLocalIndexSetMap and the constraint indexing of
+ * dftUtils::constraintMatrixInfo, InverseDFTSolverFunction.cpp:281-283 and
+ * MultiVectorAdjointLinearSolverProblem.cpp:476-538).  `n` must equal the
+ * map's length (BAD_ARG otherwise, with the length in the message).
+ *   CELL_NODES   [n_cells*n1^3] node of each cell entry
+ *   CELL_GATHER  [n_cells*n1^3] that node when it is free, else -(1 + r), r its
+ *                row in the psi constraints (the gather of the Lowdin HX)
+ *   CELL_SLOTS   [n_cells*n1^3] slot of the entry in the cell-result layout
+ *                (-1: a Dirichlet row, dropped)
+ *   *_ROWS/_PTR/_MASTERS  closed CSR of the psi, adjoint and child constraints
+ *   CHILD_CELL_NODES [n_child_cells*8], PQ_CHILD [n_cells*n1^3] */
+enum {
+  INVDFT_MAP_CELL_NODES = 0, INVDFT_MAP_CELL_GATHER = 1, INVDFT_MAP_CELL_SLOTS = 2,
+  INVDFT_MAP_PSI_ROWS = 3, INVDFT_MAP_PSI_PTR = 4, INVDFT_MAP_PSI_MASTERS = 5,
+  INVDFT_MAP_ADJ_ROWS = 6, INVDFT_MAP_ADJ_PTR = 7, INVDFT_MAP_ADJ_MASTERS = 8,
+  INVDFT_MAP_CHILD_ROWS = 9, INVDFT_MAP_CHILD_PTR = 10, INVDFT_MAP_CHILD_MASTERS = 11,
+  INVDFT_MAP_CHILD_CELL_NODES = 12, INVDFT_MAP_PQ_CHILD = 13
+};
+invdft_status invdft_get_index_map(invdft_ctx *ctx, int32_t which, int32_t *out, int64_t n);
+
 /* L-BFGS driver of BFGSInverseDFTSolver::solve with the CP line search
  * (BFGSInverseDFTSolver.cpp:467-627).  pot is updated in place; losses
  * [2*max_iter+1] (may be NULL) receives the loss of each force evaluation

@@ -294,6 +294,41 @@ invdft_status invdft_adjoint_solve(invdft_ctx *ctx, double *d_x, double tol, int
   });
 }
 
+invdft_status invdft_get_index_map(invdft_ctx *ctx, int32_t which, int32_t *out, int64_t n) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!out || n < 0) throw invdft::StatusError(INVDFT_BAD_ARG, "null output or negative length");
+    const invdft::DevBuf<int> *src = nullptr;
+    int64_t len = 0;
+    auto cons = [&](const invdft::Cons &k, int part) {
+      if (part == 0) { src = &k.rows; len = k.n; }
+      else if (part == 1) { src = &k.ptr; len = k.n + 1; }
+      else { src = &k.masters; len = k.n ? (int64_t)k.h_nnz : 0; }
+    };
+    switch (which) {
+      case INVDFT_MAP_CELL_NODES: src = &c.cell_nodes; len = c.nc * c.nd; break;
+      case INVDFT_MAP_CELL_GATHER: src = &c.cell_map; len = c.nc * c.nd; break;
+      case INVDFT_MAP_CELL_SLOTS: src = &c.d_slot_of; len = c.nc * c.nd; break;
+      case INVDFT_MAP_PSI_ROWS: cons(c.cpsi, 0); break;
+      case INVDFT_MAP_PSI_PTR: cons(c.cpsi, 1); break;
+      case INVDFT_MAP_PSI_MASTERS: cons(c.cpsi, 2); break;
+      case INVDFT_MAP_ADJ_ROWS: cons(c.cadj, 0); break;
+      case INVDFT_MAP_ADJ_PTR: cons(c.cadj, 1); break;
+      case INVDFT_MAP_ADJ_MASTERS: cons(c.cadj, 2); break;
+      case INVDFT_MAP_CHILD_ROWS: cons(c.cchild, 0); break;
+      case INVDFT_MAP_CHILD_PTR: cons(c.cchild, 1); break;
+      case INVDFT_MAP_CHILD_MASTERS: cons(c.cchild, 2); break;
+      case INVDFT_MAP_CHILD_CELL_NODES: src = &c.ch_nodes; len = c.ncc * 8; break;
+      case INVDFT_MAP_PQ_CHILD: src = &c.pq_child; len = c.nc * c.nq; break;
+      default: throw invdft::StatusError(INVDFT_BAD_ARG, "unknown index map");
+    }
+    if (n != len)
+      throw invdft::StatusError(INVDFT_BAD_ARG, "index map length is " + std::to_string(len) + ", not " +
+                                                    std::to_string(n));
+    if (len) src->download(out, (size_t)len, c.stream);
+    INVDFT_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
 invdft_status invdft_bfgs_solve(invdft_ctx *ctx, double *pot, int32_t max_iter, double tol,
                                 int32_t line_search_iters, double line_search_tol, int32_t history,
                                 double *losses, int32_t *n_evals) {

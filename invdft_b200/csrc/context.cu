@@ -58,6 +58,7 @@ void upload_cons(Cons &c, const invdft_constraints &h, int64_t nnodes, cudaStrea
   }
   for (int64_t r = 0; r <= h.n_rows; ++r) ptr[r] = (int)h.ptr[r];
   const int64_t nm = h.n_rows ? h.ptr[h.n_rows] : 0;
+  c.h_nnz = nm;
   std::vector<int> m(nm);
   for (int64_t k = 0; k < nm; ++k) {
     check(h.masters[k] >= 0 && h.masters[k] < nnodes, "constraint master out of range");

@@ -18,6 +18,7 @@ struct Cons {                      // device copy of a closed constraint set
   DevBuf<int> rows, ptr, masters;
   DevBuf<double> w;
   std::vector<int64_t> h_rows;     // host copy of the constrained rows
+  int64_t h_nnz = 0;               // master entries
 };
 
 struct Timer {

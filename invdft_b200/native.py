@@ -25,8 +25,13 @@ EXPORTED = [
     "invdft_adjoint_vmult", "invdft_adjoint_precondition_jacobi",
     "invdft_adjoint_precondition_jacobi_sqrt", "invdft_adjoint_distribute_x", "invdft_adjoint_solve",
     "invdft_bfgs_solve", "invdft_coldot_noalloc", "invdft_project_vxc_to_parent", "invdft_evaluate_parent_field",
-    "invdft_force_backward_at", "invdft_dot_blocks",
+    "invdft_force_backward_at", "invdft_dot_blocks", "invdft_get_index_map",
 ]
+
+# invdft_get_index_map selectors (include/invdft_force.h)
+INDEX_MAPS = {"cell_nodes": 0, "cell_gather": 1, "cell_slots": 2, "psi_rows": 3, "psi_ptr": 4, "psi_masters": 5,
+              "adj_rows": 6, "adj_ptr": 7, "adj_masters": 8, "child_rows": 9, "child_ptr": 10,
+              "child_masters": 11, "child_cell_nodes": 12, "pq_child": 13}
 
 
 class InvDFTError(RuntimeError):
@@ -118,6 +123,7 @@ def load() -> C.CDLL:
         "invdft_force_backward": (C.c_int, [vp, _f64p, _P(Stats)]),
         "invdft_force_backward_at": (C.c_int, [vp, C.c_int64, _f64p, _P(Stats)]),
         "invdft_dot_blocks": (C.c_int, [vp, _f64p, _f64p, C.c_int64, C.c_int32, _f64p]),
+        "invdft_get_index_map": (C.c_int, [vp, C.c_int32, _P(C.c_int32), C.c_int64]),
         "invdft_set_potential": (C.c_int, [vp, _f64p]),
         "invdft_hx": (C.c_int, [vp, vp, vp, C.c_int32]),
         "invdft_project_vxc_to_parent": (C.c_int, [vp, _f64p, _f64p]),

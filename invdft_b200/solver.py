@@ -139,6 +139,13 @@ class InverseDFTSolverFunction:
         _check(self.lib, self.ctx, self.lib.invdft_get_child_quad_products(self.ctx, ptr(out)))
         return out
 
+    def index_map(self, name: str, n: int) -> np.ndarray:
+        """An integer index map the library built on the device (int32),
+        see invdft_get_index_map."""
+        out = np.zeros(int(n), dtype=np.int32)
+        _check(self.lib, self.ctx, self.lib.invdft_get_index_map(self.ctx, native.INDEX_MAPS[name], ptr(out), int(n)))
+        return out
+
     def set_potential(self, pot):
         pot = f64(pot).copy()
         _check(self.lib, self.ctx, self.lib.invdft_set_potential(self.ctx, ptr(pot)))

@@ -185,6 +185,74 @@ def hx_probe(args, dev):
     fn.close()
 
 
+def reachable_target(P):
+    """rho* from an FP64 forward solve at v_xc* on the GPU (the configurations'
+    reachable target); installs it in P."""
+    from invdft_b200 import native
+    from invdft_b200.problem.system import set_target_density
+    from invdft_b200.solver import InverseDFTSolverFunction
+    fwd = InverseDFTSolverFunction(P, native.default_params(cheb_degree=0, cheby_tol=1e-9, initial_tol_cheb=1e-9,
+                                                            max_cheb_passes=200))
+    fwd.solve_eigen(P.vxc_exact.copy())
+    _, occ, _ = fwd.eigen()
+    psi = fwd.psi()
+    rho_q = fwd.density()
+    fwd.close()
+    set_target_density(P, rho_q, 2.0 * np.sum(occ[None, :] * psi * psi, axis=1))
+
+
+def converge(args):
+    """The metric as defined: L-BFGS (CP line search) from the Fermi-Amaldi
+    guess until int |rho - rho*| <= --converge-target, with the reachable target
+    of the configuration, in FP64 and in MIXED precision; device time with CUDA
+    events.  Reports evaluations, iterations and time to the target, and the
+    final v_xc of the two runs against each other."""
+    import torch
+    from invdft_b200.problem.system import build_problem
+    from invdft_b200.solver import InverseDFTSolverFunction, bfgs_run
+    P = build_problem(args.config, target_solver="atoms")
+    reachable_target(P)
+    runs = {}
+    for prec in ("fp64", "mixed"):
+        fn = InverseDFTSolverFunction(P, force_params(prec))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        v, rep, losses, l1 = bfgs_run(fn, P.vxc_init.copy(), args.converge_max_iter,
+                                      density_l1_target=args.converge_target)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        runs[prec] = dict(report=rep, ms=ms, evals_per_s=rep["n_evals"] / (ms / 1000.0),
+                          density_l1_first_last=[float(l1[0]), float(l1[-1])], v=v)
+        fn.close()
+    v64, vmx = runs["fp64"].pop("v"), runs["mixed"].pop("v")
+    free = np.ones(P.n_child_nodes, dtype=bool)
+    free[P.cons_child.nodes] = False
+    out = {"mode": "converge", "workload": workload_name(args.config, P, "fp64 and mixed"),
+           "target": f"int |rho - rho*| <= {args.converge_target:g} (reachable rho* from an FP64 forward solve)",
+           "runs": runs,
+           "time_to_target_speedup_mixed_vs_fp64": runs["fp64"]["ms"] / runs["mixed"]["ms"],
+           "evals_per_s_ratio_mixed_vs_fp64": runs["mixed"]["evals_per_s"] / runs["fp64"]["evals_per_s"],
+           "final_vxc_rel_l2_mixed_vs_fp64": float(np.linalg.norm((vmx - v64)[free]) / np.linalg.norm(v64[free]))}
+    print(json.dumps(out))
+
+
+def kernel_probe(args):
+    """One launch of each kernel of the evaluation on the workload's full-size
+    buffers (invdft_kernel_probe): the launch sequence the per-kernel profiles
+    in profiles/ are captured on, with few launches before each."""
+    from invdft_b200.problem.system import build_problem
+    from invdft_b200.solver import InverseDFTSolverFunction, _check
+    P = build_problem(args.config, target_solver="atoms")
+    fn = InverseDFTSolverFunction(P, force_params("fp64"))
+    fn.set_potential(P.vxc_init.copy())
+    for _ in range(max(args.steps, 1)):
+        _check(fn.lib, fn.ctx, fn.lib.invdft_kernel_probe(fn.ctx))
+    print(json.dumps({"probe": "kernels", "workload": args.config, "n_dofs": P.n_nodes, "rounds": max(args.steps, 1)}))
+    fn.close()
+
+
 def aggregate(ms: float, e2e_s: float, steps: int, world: int, dist=None, device="cuda"):
     """Whole-job throughput of ``world`` replicas timed as the max over ranks.
 
@@ -279,6 +347,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU evaluation (profiling runs)")
     ap.add_argument("--ref-budget-s", type=float, default=240.0,
                     help="reference arm: stop timing CPU evaluations once this much time is spent")
+    ap.add_argument("--converge", action="store_true",
+                    help="L-BFGS to a fixed int |rho - rho*| in FP64 and MIXED precision (the metric as defined)")
+    ap.add_argument("--converge-target", type=float, default=1e-5)
+    ap.add_argument("--converge-max-iter", type=int, default=300)
+    ap.add_argument("--kernel-probe", action="store_true",
+                    help="profiling: one launch of each kernel of the evaluation on the workload's buffers")
     ap.add_argument("--hx-width", type=str, default="0",
                     help="kernel probe for profiling: --steps Lowdin HX applications of a seeded block of this "
                          "width at v_xc = the initial guess, timed with CUDA events (no force evaluation)")
@@ -307,6 +381,12 @@ def main():
 
     if args.hx_width != "0":
         hx_probe(args, dev)
+        return
+    if args.kernel_probe:
+        kernel_probe(args)
+        return
+    if args.converge:
+        converge(args)
         return
 
     P, info = build_workload(args.config)

@@ -4,10 +4,12 @@
  * The library replaces, for one GPU, the reference's
  *   InverseDFTSolverFunction<p,pe,mem>          (include/InverseDFTSolverFunction.h:51-384)
  *   MultiVectorAdjointLinearSolverProblem<mem>  (include/MultiVectorAdjointLinearSolverProblem.h:15-214)
- * behind plain pointers and sizes.  All arithmetic on the path is FP64.  With
- * INVDFT_PRECISION_MIXED the Chebyshev filter streams the cell matrices stored
- * in FP32 (products still accumulated in FP64 on the tensor cores) until the
- * residual reaches mixed_residual_floor; everything else stays FP64.
+ * behind plain pointers and sizes.  All arithmetic on the path is FP64 by
+ * default.  With INVDFT_PRECISION_MIXED the early Chebyshev passes run FP32
+ * cell products until the residual reaches mixed_residual_floor, and the
+ * adjoint block MINRES runs on FP32 cell products inside an FP64 iterative
+ * refinement (FP64 true residuals, FP64 Lanczos scalars); Rayleigh-Ritz,
+ * Cholesky, densities, transfers and the force stay FP64.
  *
  * Vectors ("multi-vectors") are row-major [n_nodes][B]: node index slowest,
  * vector index fastest, as the reference's dftfe::linearAlgebra::MultiVector
@@ -111,8 +113,11 @@ typedef struct {
   double factor_lda;              /* FACTOR FOR LDA VXC */
   int32_t lanczos_steps;          /* steps of the spectrum-bound Lanczos run */
   int32_t precision;              /* invdft_precision */
-  double mixed_residual_floor;    /* MIXED: filter with FP32-stored cell matrices until the max
+  double mixed_residual_floor;    /* MIXED: filter with FP32 cell products until the max
                                      residual falls below this or stalls, then in FP64 */
+  double mixed_inner_tol;         /* MIXED: relative tolerance of each FP32-operator MINRES solve
+                                     inside the FP64 iterative refinement of the adjoint problem */
+  int32_t mixed_max_refine;       /* MIXED: refinement steps at most (each computes the FP64 true residual) */
 } invdft_params;
 
 typedef struct {
@@ -145,6 +150,7 @@ typedef struct {
   int32_t passes_low;        /* Chebyshev passes filtered with FP32-stored cell matrices */
   int64_t generation;        /* state generation of the forward half this evaluation ran (see
                                 invdft_force_backward_at) */
+  int32_t refine_steps;      /* MIXED: FP64 refinement steps of the adjoint solves */
 } invdft_force_stats;
 
 /* Defaults of the reference's parameters. */
@@ -261,6 +267,62 @@ invdft_status invdft_adjoint_distribute_x(invdft_ctx *ctx, double *d_x);
 invdft_status invdft_adjoint_solve(invdft_ctx *ctx, double *d_x, double tol, int32_t max_iter,
                                    int32_t *iters);
 
+/* The base potential v_base on the GPU: InverseDFTEngine::setPotBasePoissonNuclear
+ * (InverseDFTEngine.cpp:2459-2571) with solvePhiTotalAllElectronNonPeriodic
+ * (:2573-2621).  Solves, on the parent mesh with its psi constraints (hanging
+ * nodes, zero boundary), the Poisson problem of the total electrostatic
+ * potential of the density rho_quad [n_cells*n1^3] (host, total at the parent
+ * quadrature points) and n_atoms point nuclei of charge Z[a] in cell
+ * atom_cell[a] at reference coordinates atom_xi[3a..3a+2] in [0, 1]^3:
+ *   -lap phi = 4 pi (rho - sum_a Z_a delta_a),
+ * by Jacobi-preconditioned CG with the matrix-free Laplacian until the
+ * residual falls below rel_tol times the right-hand side (2-norms, in the
+ * Lowdin-scaled unknowns) or max_iter.  phi_quad [n_cells*n1^3] receives phi at
+ * the quadrature points and phi_nodal [n_nodes] (may be NULL) the nodal
+ * solution; *iters and *rel_res (may be NULL) the CG iterations and final
+ * relative residual.  install != 0 makes phi_quad the context's v_base for the
+ * following evaluations (and ends the validity of the last forward half).
+ * MAXITER when max_iter ran out (results are returned). */
+invdft_status invdft_poisson_total_potential(invdft_ctx *ctx, const double *rho_quad, int32_t n_atoms,
+                                             const double *Z, const int64_t *atom_cell, const double *atom_xi,
+                                             double rel_tol, int32_t max_iter, int32_t install,
+                                             double *phi_quad, double *phi_nodal, int32_t *iters,
+                                             double *rel_res);
+
+/* One launch of each kernel of the evaluation on the context's full-size
+ * buffers, for kernel profiles (needs invdft_set_potential first): the Lowdin
+ * HX chain on the start block, the density, psi.p at the child quadrature
+ * points, the force projection, the adjoint rhs chain and one MINRES update
+ * pair.  Results are meaningless; ends the validity of the last forward half. */
+invdft_status invdft_kernel_probe(invdft_ctx *ctx);
+
+/* The initial v_xc guess on the GPU: InverseDFTEngine::setInitialPotL2Proj
+ * (InverseDFTEngine.cpp:1046-1498).  From the total target density rho_quad
+ * [n_cells*n1^3] (host, parent quadrature points) and, for LB94 exchange, its
+ * |grad rho|^2 sigma_quad (NULL: LDA exchange), forms at the quadrature points
+ *   v = (1 - p) v_x + p (v_x + v_c),  p = rho / (rho + tau_vx),
+ * with the Fermi-Amaldi far field v = q v - (1 - q) factor_fa / N_e v_H,
+ * q = rho / (rho + tau_fa), when fermi_amaldi_bc != 0 (v_H: the Hartree
+ * potential of rho solved on the GPU, boundary values hartree_bc [n_nodes] on
+ * the Dirichlet rows of the psi constraints, as computeHartreePotOnParentQuad
+ * sets them, :1790-2118).  v is L2-projected onto the parent nodes (lumped
+ * mass, psi constraints distributed), evaluated at the child Gauss points,
+ * scaled by 1 - factor_lda and L2-projected onto the child nodes, whose
+ * constrained entries are set to zero.  vxc_child [n_child_nodes] receives the
+ * guess; vxc_parent [n_nodes] and vh_quad [n_cells*n1^3] (may be NULL) the
+ * parent nodal field and v_H. */
+typedef struct {
+  double tau_vx;               /* TAU FOR WEIGHTS FOR SETTING VX BC (reference default 1e-2) */
+  double tau_fa;               /* TAU FOR WEIGHTS FOR SETTING FABC (1e-2) */
+  int32_t fermi_amaldi_bc;     /* SET FERMIAMALDI IN THE FAR FIELD AS INPUT (0) */
+  double factor_fa;            /* FACTOR FOR FERMIAMALDI (1) */
+  double hartree_rel_tol;      /* CG tolerance of the Hartree solve (relative residual) */
+  int32_t hartree_max_iter;
+} invdft_initial_guess_options;
+invdft_status invdft_initial_guess(invdft_ctx *ctx, const double *rho_quad, const double *sigma_quad,
+                                   const double *hartree_bc, const invdft_initial_guess_options *opts,
+                                   double *vxc_child, double *vxc_parent, double *vh_quad);
+
 /* Integer index data the library built on the device from the descriptor,
  * downloaded as int32 for exact comparison with the caller's (the reference's
  * cell->DoF maps of computeCellLocalIndexSetMap and the constraint indexing of
@@ -290,6 +352,30 @@ invdft_status invdft_get_index_map(invdft_ctx *ctx, int32_t which, int32_t *out,
 invdft_status invdft_bfgs_solve(invdft_ctx *ctx, double *pot, int32_t max_iter, double tol,
                                 int32_t line_search_iters, double line_search_tol,
                                 int32_t history, double *losses, int32_t *n_evals);
+
+/* The same L-BFGS driver with a stop on the density error, for runs to a
+ * fixed int |rho - rho*| (the reference stops on the force norm and the
+ * iteration cap only).  After each accepted iterate (and at the start) the run
+ * stops once int |rho - rho*| = 2 stats.l1_error <= density_l1_target (0: off).
+ * losses and density_l1 (may be NULL) receive, per force evaluation, L and
+ * int |rho - rho*|, up to `capacity` entries. */
+typedef struct {
+  int32_t max_iter;
+  double tol;                 /* force-norm tolerance */
+  int32_t line_search_iters;
+  double line_search_tol;
+  int32_t history;
+  double density_l1_target;
+} invdft_bfgs_options;
+typedef struct {
+  int32_t n_iters;            /* accepted iterates */
+  int32_t n_evals;            /* force evaluations, line-search probes included */
+  double final_loss;
+  double final_density_l1;    /* int |rho - rho*| at the last evaluation */
+  int32_t reached;            /* 1 when the density target stopped the run */
+} invdft_bfgs_report;
+invdft_status invdft_bfgs_run(invdft_ctx *ctx, double *pot, const invdft_bfgs_options *opts, double *losses,
+                              double *density_l1, int32_t capacity, invdft_bfgs_report *report);
 
 /* Per-column dot products out[j] = sum_i a[i*B+j] b[i*B+j] of device blocks
  * [n][B], computed on `stream` (a cudaStream_t, NULL = default stream) without

@@ -20,10 +20,14 @@ double dot(const std::vector<double> &a, const std::vector<double> &b) {
 }
 }  // namespace
 
-invdft_status bfgs_solve(invdft_ctx *ctx, double *pot, int max_iter, double tol, int ls_iters, double ls_tol,
-                         int history, double *losses, int *n_evals) {
+invdft_status bfgs_run(invdft_ctx *ctx, double *pot, const invdft_bfgs_options &o, double *losses,
+                       double *density_l1, int cap, invdft_bfgs_report *rep) {
+  const int max_iter = o.max_iter, ls_iters = o.line_search_iters, history = o.history;
+  const double tol = o.tol, ls_tol = o.line_search_tol;
   invdft_force_stats st;
   double L = 0.0;
+  int iters_done = 0;
+  bool reached = false;
   std::vector<double> x, g, p, s, y, xnew, gtmp;
   std::deque<std::vector<double>> Ys, Ss;
   std::deque<double> rhos;
@@ -36,15 +40,23 @@ invdft_status bfgs_solve(invdft_ctx *ctx, double *pot, int max_iter, double tol,
   // potential in place, as getForceVector does with the BFGS iterate
   auto eval = [&](std::vector<double> &xin, std::vector<double> &gout, double &Lout) -> invdft_status {
     invdft_status rc = invdft_force_eval(ctx, xin.data(), gout.data(), &Lout, &st);
-    if (losses && evals < 2 * max_iter + 1) losses[evals] = Lout;
+    if (losses && evals < cap) losses[evals] = Lout;
+    // int |rho - rho*| = 2 sum |rho*_up - rho/2| JxW in the spin-unpolarised case
+    if (density_l1 && evals < cap) density_l1[evals] = 2.0 * st.l1_error;
     ++evals;
     return rc;
   };
+  // the density target, checked at the accepted iterates (not at line-search probes)
+  auto at_target = [&]() { return o.density_l1_target > 0.0 && 2.0 * st.l1_error <= o.density_l1_target; };
   invdft_status rc = INVDFT_OK;
   for (int iter = 0; iter < max_iter; ++iter) {
     if (iter == 0) {
       rc = eval(x, g, L);
       if (rc != INVDFT_OK) break;
+      if (at_target()) {
+        reached = true;
+        break;
+      }
     }
     const double gnorm = std::sqrt(dot(g, g));
     // two-loop recursion (:68-118)
@@ -101,6 +113,8 @@ invdft_status bfgs_solve(invdft_ctx *ctx, double *pot, int max_iter, double tol,
     for (auto &v : y) v = -v;
     rc = eval(x, g, L);
     if (rc != INVDFT_OK) break;
+    iters_done = iter + 1;
+    const double l1_now = 2.0 * st.l1_error;
     for (int64_t t = 0; t < n; ++t) y[t] += g[t];
     const double curv = dot(y, s);
     if (curv > 0.0) {
@@ -115,9 +129,34 @@ invdft_status bfgs_solve(invdft_ctx *ctx, double *pot, int max_iter, double tol,
       Ss.pop_front();
       rhos.pop_front();
     }
+    if (o.density_l1_target > 0.0 && l1_now <= o.density_l1_target) {
+      reached = true;
+      break;
+    }
   }
   for (int64_t t = 0; t < n; ++t) pot[t] = x[t];
-  if (n_evals) *n_evals = evals;
+  if (rep) {
+    rep->n_iters = iters_done;
+    rep->n_evals = evals;
+    rep->final_loss = L;
+    rep->final_density_l1 = 2.0 * st.l1_error;
+    rep->reached = reached ? 1 : 0;
+  }
+  return rc;
+}
+
+invdft_status bfgs_solve(invdft_ctx *ctx, double *pot, int max_iter, double tol, int ls_iters, double ls_tol,
+                         int history, double *losses, int *n_evals) {
+  invdft_bfgs_options o{};
+  o.max_iter = max_iter;
+  o.tol = tol;
+  o.line_search_iters = ls_iters;
+  o.line_search_tol = ls_tol;
+  o.history = history;
+  o.density_l1_target = 0.0;
+  invdft_bfgs_report rep{};
+  const invdft_status rc = bfgs_run(ctx, pot, o, losses, nullptr, 2 * max_iter + 1, &rep);
+  if (n_evals) *n_evals = rep.n_evals;
   return rc;
 }
 

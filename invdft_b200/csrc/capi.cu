@@ -44,6 +44,8 @@ void set_thread_error(const std::string &msg) { g_create_error = msg; }
 // Implemented in bfgs.cpp
 invdft_status bfgs_solve(invdft_ctx *ctx, double *pot, int max_iter, double tol, int ls_iters, double ls_tol,
                          int history, double *losses, int *n_evals);
+invdft_status bfgs_run(invdft_ctx *ctx, double *pot, const invdft_bfgs_options &o, double *losses,
+                       double *density_l1, int cap, invdft_bfgs_report *rep);
 }
 
 extern "C" {
@@ -68,6 +70,8 @@ void invdft_default_params(invdft_params *p) {
   p->lanczos_steps = 20;
   p->precision = INVDFT_PRECISION_FP64;
   p->mixed_residual_floor = 1e-4;
+  p->mixed_inner_tol = 1e-4;
+  p->mixed_max_refine = 12;
 }
 
 invdft_status invdft_force_create(const invdft_problem_desc *desc, const invdft_params *params,
@@ -294,6 +298,44 @@ invdft_status invdft_adjoint_solve(invdft_ctx *ctx, double *d_x, double tol, int
   });
 }
 
+invdft_status invdft_poisson_total_potential(invdft_ctx *ctx, const double *rho_quad, int32_t n_atoms,
+                                             const double *Z, const int64_t *atom_cell, const double *atom_xi,
+                                             double rel_tol, int32_t max_iter, int32_t install,
+                                             double *phi_quad, double *phi_nodal, int32_t *iters,
+                                             double *rel_res) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!rho_quad || (n_atoms > 0 && (!Z || !atom_cell || !atom_xi)))
+      throw invdft::StatusError(INVDFT_BAD_ARG, "null density or atom arrays");
+    int it = 0;
+    double res = 0.0;
+    try {
+      c.poisson_total(rho_quad, n_atoms, Z, atom_cell, atom_xi, rel_tol, max_iter, install != 0, phi_quad,
+                      phi_nodal, &it, &res);
+    } catch (...) {
+      if (iters) *iters = it;
+      if (rel_res) *rel_res = res;
+      throw;
+    }
+    if (iters) *iters = it;
+    if (rel_res) *rel_res = res;
+  });
+}
+
+invdft_status invdft_initial_guess(invdft_ctx *ctx, const double *rho_quad, const double *sigma_quad,
+                                   const double *hartree_bc, const invdft_initial_guess_options *opts,
+                                   double *vxc_child, double *vxc_parent, double *vh_quad) {
+  return guard(ctx, [&](invdft::Context &c) {
+    if (!rho_quad || !opts || !vxc_child) throw invdft::StatusError(INVDFT_BAD_ARG, "null density, options or output");
+    if (opts->fermi_amaldi_bc && !hartree_bc)
+      throw invdft::StatusError(INVDFT_BAD_ARG, "the Fermi-Amaldi far field needs the Hartree boundary values");
+    c.initial_guess(rho_quad, sigma_quad, hartree_bc, *opts, vxc_child, vxc_parent, vh_quad);
+  });
+}
+
+invdft_status invdft_kernel_probe(invdft_ctx *ctx) {
+  return guard(ctx, [&](invdft::Context &c) { c.kernel_probe(); });
+}
+
 invdft_status invdft_get_index_map(invdft_ctx *ctx, int32_t which, int32_t *out, int64_t n) {
   return guard(ctx, [&](invdft::Context &c) {
     if (!out || n < 0) throw invdft::StatusError(INVDFT_BAD_ARG, "null output or negative length");
@@ -335,6 +377,13 @@ invdft_status invdft_bfgs_solve(invdft_ctx *ctx, double *pot, int32_t max_iter, 
   if (!ctx || !ctx->c || !pot || max_iter < 0 || history < 1) return INVDFT_BAD_ARG;
   return invdft::bfgs_solve(ctx, pot, max_iter, tol, line_search_iters, line_search_tol, history, losses,
                             n_evals);
+}
+
+invdft_status invdft_bfgs_run(invdft_ctx *ctx, double *pot, const invdft_bfgs_options *opts, double *losses,
+                              double *density_l1, int32_t capacity, invdft_bfgs_report *report) {
+  if (!ctx || !ctx->c || !pot || !opts || opts->max_iter < 0 || opts->history < 1 || capacity < 0)
+    return INVDFT_BAD_ARG;
+  return invdft::bfgs_run(ctx, pot, *opts, losses, density_l1, capacity, report);
 }
 
 }  // extern "C"

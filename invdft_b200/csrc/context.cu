@@ -59,6 +59,9 @@ void upload_cons(Cons &c, const invdft_constraints &h, int64_t nnodes, cudaStrea
   for (int64_t r = 0; r <= h.n_rows; ++r) ptr[r] = (int)h.ptr[r];
   const int64_t nm = h.n_rows ? h.ptr[h.n_rows] : 0;
   c.h_nnz = nm;
+  c.h_ptr.assign(h.ptr, h.ptr + h.n_rows + 1);
+  c.h_masters.assign(h.masters, h.masters + nm);
+  c.h_w.assign(h.weights, h.weights + nm);
   std::vector<int> m(nm);
   for (int64_t k = 0; k < nm; ++k) {
     check(h.masters[k] >= 0 && h.masters[k] < nnodes, "constraint master out of range");
@@ -430,6 +433,7 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   d_err.zero(s);
   sqrtM.upload(sm, s);
   invsqrtM.upload(ism, s);
+  h_invsqrtM = ism;
   diagA.upload(dA, s);
   diagSqrtA.upload(dSA, s);
 
@@ -533,6 +537,8 @@ void Context::set_params(const invdft_params *pp) {
   check(pp->lanczos_steps >= 2, "lanczos_steps must be >= 2");
   check(pp->precision == INVDFT_PRECISION_FP64 || pp->precision == INVDFT_PRECISION_MIXED, "bad precision");
   check(pp->mixed_residual_floor >= 0.0, "mixed_residual_floor must be >= 0");
+  check(pp->mixed_inner_tol > 0.0 && pp->mixed_inner_tol < 1.0, "mixed_inner_tol must be in (0, 1)");
+  check(pp->mixed_max_refine >= 1, "mixed_max_refine must be >= 1");
   prm = *pp;
 }
 
@@ -1143,9 +1149,96 @@ __global__ void scatter_columns_kernel(const double *__restrict__ src, int bsrc,
 // uncompacted solve.
 void Context::adj_minres(double *d_x, double tol, int maxit, std::vector<int> &iters) {
   if (!psi_ready) throw StatusError(INVDFT_NOT_READY, "updateInputPsi has not been called");
+  adj_compute_rhs(m_b.p);
+  if (prm.precision == INVDFT_PRECISION_MIXED) minres_refined(m_b.p, d_x, tol, maxit, iters);
+  else minres_core(m_b.p, d_x, tol, maxit, iters, false);
+  last_iters = iters;
+  adj_distribute_x(d_x);
+}
+
+namespace {
+__global__ void scale_columns_kernel(double *x, const double *s, int64_t n, int B) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n * B) x[i] *= s[i % B];
+}
+__global__ void add_scaled_columns_kernel(double *x, const double *d, const double *s, int64_t n, int B) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n * B) x[i] = fma(s[i % B], d[i], x[i]);
+}
+}  // namespace
+
+// The precision form of the adjoint solve: iterative refinement in FP64 around
+// block MINRES whose operator applications use the FP32 matrix-free cell
+// product.  Each step takes the FP64 true residual r = b - A x (A the FP64
+// vmult operator), its preconditioned norm |r|_D = sqrt(r^T D r) per column,
+// stops the columns below tol, and solves A d = r / |r|_D with FP32 cell
+// products to the relative tolerance mixed_inner_tol (FP64 Lanczos scalars and
+// vectors), then x += |r|_D d.  The refinement converges while the FP32
+// operator error (~6e-8 lambda_max) stays below the smallest |eigenvalue| of
+// (H - eps_i) the right-hand side reaches; iteration counts are the sums over
+// the inner solves.
+void Context::minres_refined(const double *d_b, double *d_x, double tol, int maxit, std::vector<int> &iters) {
   const int Bw = B;
   const size_t v = (size_t)nn * Bw;
-  adj_compute_rhs(m_b.p);
+  DevBuf<double> r(v), d(v), sc(Bw);
+  INVDFT_CUDA(cudaMemsetAsync(d_x, 0, v * sizeof(double), stream));
+  INVDFT_CUDA(cudaMemcpyAsync(r.p, d_b, v * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+  iters.assign(Bw, 0);
+  std::vector<double> nrm(Bw), s(Bw);
+  std::vector<int> its;
+  int used = 0;
+  for (int step = 0; step < prm.mixed_max_refine && used < maxit; ++step) {
+    // |r|_D per column
+    launch_scale_rows(diagA.p, r.p, d.p, nn, Bw, stream);
+    launch_coldot(r.p, d.p, nn, Bw, partial.p, nblocks_red, small.p, stream);
+    INVDFT_CUDA(cudaMemcpyAsync(nrm.data(), small.p, sizeof(double) * Bw, cudaMemcpyDeviceToHost, stream));
+    INVDFT_CUDA(cudaStreamSynchronize(stream));
+    bool any = false;
+    for (int j = 0; j < Bw; ++j) {
+      nrm[j] = std::sqrt(std::max(nrm[j], 0.0));
+      if (!std::isfinite(nrm[j])) throw StatusError(INVDFT_NONFINITE, "non-finite adjoint residual");
+      const bool act = nrm[j] >= tol;
+      s[j] = act ? 1.0 / nrm[j] : 0.0;
+      any = any || act;
+    }
+    if (!any) break;
+    sc.upload(s, stream);
+    scale_columns_kernel<<<ceil_div((int64_t)v, 256), 256, 0, stream>>>(r.p, sc.p, nn, Bw);
+    INVDFT_LAUNCH_CHECK();
+    count_launch();
+    minres_core(r.p, d.p, prm.mixed_inner_tol, maxit - used, its, true);
+    int most = 0;
+    for (int j = 0; j < Bw; ++j) {
+      iters[j] += its[j];
+      most = std::max(most, its[j]);
+    }
+    used += std::max(most, 1);
+    for (int j = 0; j < Bw; ++j) s[j] = s[j] > 0.0 ? nrm[j] : 0.0;
+    sc.upload(s, stream);
+    add_scaled_columns_kernel<<<ceil_div((int64_t)v, 256), 256, 0, stream>>>(d_x, d.p, sc.p, nn, Bw);
+    INVDFT_LAUNCH_CHECK();
+    count_launch();
+    // FP64 true residual r = b - A x (vmult operator: constrained rows zero)
+    cell_gemm(d_x, Bw);
+    AsmEpilogue epi;
+    epi.kind = AsmEpilogue::VMULT;
+    epi.eps = a_eig.p;
+    epi.in = d_x;
+    launch_hx_assemble(fe, Ycell.p, r.p, Bw, epi, 0, stream);
+    launch_set_zero(cpsi.rows.p, cpsi.n, r.p, Bw, stream);
+    n_hx++;
+    n_hx_cols += Bw;
+    lincomb(r.p, -1.0, r.p, 1.0, d_b, 0.0, nullptr, (int64_t)v, stream);
+    ++refine_steps;
+  }
+}
+
+// Block MINRES on A x = rhs from x = 0, per-column convergence at |r|_D < tol;
+// low: the operator applications use the FP32 matrix-free cell product.
+void Context::minres_core(const double *d_rhs, double *d_x, double tol, int maxit, std::vector<int> &iters,
+                          bool low) {
+  const int Bw = B;
+  const size_t v = (size_t)nn * Bw;
   INVDFT_CUDA(cudaMemsetAsync(d_x, 0, v * sizeof(double), stream));
   MinresState st;
   double *sc = m_scal.p;
@@ -1159,7 +1252,7 @@ void Context::adj_minres(double *d_x, double tol, int maxit, std::vector<int> &i
     const size_t need = (size_t)assemble_blocks(fe, Bw) * Bw;
     if (partial.n < need) partial.alloc(need);
   }
-  launch_minres_init(m_b.p, diagA.p, m_r1.p, m_r2.p, m_y.p, nn, Bw, partial.p, nblocks_red, stream);
+  launch_minres_init(d_rhs, diagA.p, m_r1.p, m_r2.p, m_y.p, nn, Bw, partial.p, nblocks_red, stream);
   launch_reduce_partials(partial.p, nblocks_red, Bw, st.beta2, stream);
   launch_minres_init_scalars(st, st.beta2, Bw, stream);
   std::vector<int> iters_full(Bw, 0);
@@ -1233,7 +1326,7 @@ void Context::adj_minres(double *d_x, double tol, int maxit, std::vector<int> &i
       if ((int)keep.size() < Bc && (4 * (int)keep.size() <= 3 * Bc || (int)keep.size() + 2 <= Bc)) compact(keep);
     }
     launch_minres_v(m_y.p, st, m_v.p, nn, Bc, stream);
-    cell_gemm(m_v.p, Bc);
+    cell_gemm(m_v.p, Bc, low && hx_variant == 3);
     AsmEpilogue epi;
     epi.kind = AsmEpilogue::MINRES;
     epi.in = m_v.p;
@@ -1255,8 +1348,45 @@ void Context::adj_minres(double *d_x, double tol, int maxit, std::vector<int> &i
   INVDFT_CUDA(cudaStreamSynchronize(stream));
   for (int k = 0; k < Bc; ++k) iters_full[cmap[k]] = it_now[k];
   iters = iters_full;
-  last_iters = iters;
-  adj_distribute_x(d_x);
+}
+
+// One launch of each kernel of the evaluation on full-size buffers, for
+// kernel profiles: the matrix-free HX chain on the start block, the density
+// with unit occupancies, psi.psi at the child quadrature points, the force
+// projection, the adjoint rhs chain and one masked MINRES update pair.  Values
+// are those of the start subspace; only the launches matter.
+void Context::kernel_probe() {
+  if (!have_H) throw StatusError(INVDFT_NOT_READY, "no potential set");
+  hx(X.p, Yb.p, N);
+  launch_scale_rows(invsqrtM.p, X.p, psi.p, nn, N, stream);
+  occ.assign(N, 1.0);
+  double sums[4];
+  density_and_loss(sums);
+  S.zero(stream);
+  accumulate_child_products(psi.p, psi.p, N);
+  launch_force_project(cv, S.p, force_d.p, stream);
+  std::vector<std::vector<int>> degen(N);
+  for (int i = 0; i < N; ++i) degen[i] = {i};
+  std::vector<double> f(N, 1.0), e(N, -0.5);
+  adj_update_psi(psi.p, N, 0, f.data(), u.p, degen, 0.0, e.data(), N);
+  adj_compute_rhs(m_b.p);
+  MinresState st;
+  double *sc = m_scal.p;
+  st.beta = sc + 0 * 64; st.oldb = sc + 1 * 64; st.dbar = sc + 2 * 64; st.epsln = sc + 3 * 64;
+  st.phibar = sc + 4 * 64; st.cs = sc + 5 * 64; st.sn = sc + 6 * 64; st.alfa = sc + 7 * 64;
+  st.beta2 = sc + 8 * 64; st.coef1 = sc + 9 * 64; st.oldeps = sc + 10 * 64; st.delta = sc + 11 * 64;
+  st.denom = sc + 12 * 64; st.phi = sc + 13 * 64;
+  st.active = m_flags.p; st.commit = m_flags.p + 64; st.iters = m_flags.p + 128;
+  std::vector<double> ones(16 * 64, 1.0);
+  std::vector<int> flags(3 * 64, 1);
+  INVDFT_CUDA(cudaMemcpyAsync(m_scal.p, ones.data(), sizeof(double) * ones.size(), cudaMemcpyHostToDevice, stream));
+  INVDFT_CUDA(cudaMemcpyAsync(m_flags.p, flags.data(), sizeof(int) * flags.size(), cudaMemcpyHostToDevice, stream));
+  m_xc.ensure((size_t)nn * N);
+  launch_minres_update1(m_r1.p, m_r2.p, m_y.p, m_b.p, diagA.p, st, nn, N, partial.p, nblocks_red, stream);
+  launch_minres_update2(m_xc.p, m_w.p, m_w2.p, m_b.p, st, nn, N, stream);
+  INVDFT_CUDA(cudaStreamSynchronize(stream));
+  invalidate_forward();
+  psi_ready = false;
 }
 
 void Context::accumulate_child_products(const double *d_psi, const double *d_p, int Bw) {
@@ -1359,6 +1489,7 @@ void Context::forward(double *pot, invdft_force_stats *st) {
 void Context::backward(double *force, invdft_force_stats *st, int64_t expected_generation) {
   if (!have_forward)
     throw StatusError(INVDFT_NOT_READY, "backward needs a forward evaluation first (or the potential changed since)");
+  refine_steps = 0;
   if (expected_generation >= 0 && expected_generation != generation)
     throw StatusError(INVDFT_NOT_READY, "the context ran another forward evaluation (or changed its potential) "
                                         "after the one this backward belongs to");
@@ -1414,6 +1545,7 @@ void Context::backward(double *force, invdft_force_stats *st, int64_t expected_g
   st->device_bytes = (double)device_bytes().load();
   st->device_bytes_peak = (double)device_bytes_peak().load();
   st->generation = generation;
+  st->refine_steps = refine_steps;
   profile_end(st);
   check_device_error();
 }

@@ -19,6 +19,8 @@ struct Cons {                      // device copy of a closed constraint set
   DevBuf<double> w;
   std::vector<int64_t> h_rows;     // host copy of the constrained rows
   int64_t h_nnz = 0;               // master entries
+  std::vector<int64_t> h_ptr, h_masters;  // host copy of the CSR
+  std::vector<double> h_w;
 };
 
 struct Timer {
@@ -69,6 +71,7 @@ class Context {
   bool needs_cell_matrices() const;
   void check_device_error();
   DevBuf<double> sqrtM, invsqrtM, diagA, diagSqrtA;
+  std::vector<double> h_invsqrtM;  // host copy of M^-1/2 (0 on constrained rows)
   std::vector<char> h_free;        // unconstrained psi rows
   // child data
   DevBuf<int> ch_nodes, ch_parent, pq_child, ch_sc_ptr, ch_sc_src, work_parent, work_c0, work_c1;
@@ -144,6 +147,9 @@ class Context {
   void adj_precondition(double *d_dst, const double *d_src, bool sqrt_version);
   void adj_distribute_x(double *d_x);
   void adj_minres(double *d_x, double tol, int maxit, std::vector<int> &iters);
+  void minres_core(const double *d_rhs, double *d_x, double tol, int maxit, std::vector<int> &iters, bool low);
+  void minres_refined(const double *d_b, double *d_x, double tol, int maxit, std::vector<int> &iters);
+  int refine_steps = 0;            // FP64 refinement steps of the adjoint solves of this evaluation
   // full evaluation = forward half + backward half
   void forward(double *pot, invdft_force_stats *st);
   // expected_generation < 0: the current forward half, whichever it is
@@ -158,6 +164,21 @@ class Context {
   double last_loss = 0.0;
   long long fwd_launches0 = 0;
   void accumulate_child_products(const double *d_psi, const double *d_p, int Bw);
+  // v_base = total electrostatic potential of a density and point nuclei
+  // (InverseDFTEngine::setPotBasePoissonNuclear), by preconditioned CG on the
+  // GPU with the matrix-free Laplacian; host arrays
+  void poisson_total(const double *h_rho_quad, int n_atoms, const double *Z, const int64_t *atom_cell,
+                     const double *atom_xi, double rel_tol, int max_iter, bool install, double *h_phi_quad,
+                     double *h_phi_nodal, int *iters, double *rel_res);
+  void poisson_solve(const double *h_rho, int n_atoms, const double *Z, const int64_t *atom_cell,
+                     const double *atom_xi, const double *h_bc, double rel_tol, int max_iter, DevBuf<double> &phi,
+                     int &it, double &res);
+  // initial v_xc guess (InverseDFTEngine::setInitialPotL2Proj); host arrays
+  void initial_guess(const double *h_rho, const double *h_sigma, const double *h_bc,
+                     const invdft_initial_guess_options &o, double *h_vxc_child, double *h_vxc_parent,
+                     double *h_vh_quad);
+  DevBuf<double> vj_zero;          // zero potential term: the cell products of the Laplacian
+  void kernel_probe();             // one launch of each kernel (profiling)
 
  private:
   void alloc_state();

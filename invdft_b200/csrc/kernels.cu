@@ -1874,6 +1874,23 @@ __global__ void mul_kernel(const double *__restrict__ a, const double *__restric
   if (i < n) out[i] = a[i] * b[i];
 }
 
+__global__ void axpbypcz_kernel(double *__restrict__ out, double a, const double *__restrict__ x, double b,
+                                const double *__restrict__ y, double c, const double *__restrict__ z, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v = a * x[i];
+  if (y) v = fma(b, y[i], v);
+  if (z) v = fma(c, z[i], v);
+  out[i] = v;
+}
+
+void launch_axpbypcz(double *out, double a, const double *x, double b, const double *y, double c, const double *z,
+                     int64_t n, cudaStream_t s) {
+  if (n == 0) return;
+  axpbypcz_kernel<<<ceil_div(n, NT), NT, 0, s>>>(out, a, x, b, y, c, z, n);
+  INVDFT_LAUNCH_CHECK();
+}
+
 void launch_mul(const double *a, const double *b, double *out, int64_t n, cudaStream_t s) {
   if (n == 0) return;
   mul_kernel<<<ceil_div(n, NT), NT, 0, s>>>(a, b, out, n);

@@ -115,6 +115,9 @@ void launch_hx_cell_sf_f32(const FeView &fe, const SfMatsT<float> &mt, const dou
                            double *Ycell, int B, int gather_mode, cudaStream_t s);
 // out[i] = a[i] * b[i]
 void launch_mul(const double *a, const double *b, double *out, int64_t n, cudaStream_t s);
+// out[i] = a x[i] + b y[i] + c z[i] (y, z may be null); out may alias x, y or z
+void launch_axpbypcz(double *out, double a, const double *x, double b, const double *y, double c, const double *z,
+                     int64_t n, cudaStream_t s);
 // bulk-asynchronous staged variant (persistent CTAs, shared-memory panel ring)
 void launch_hx_cell_gemm_bulk(const FeView &fe, const double *H, const double *x, double *Yslot, int B,
                               int gather_mode, cudaStream_t s);

@@ -26,6 +26,7 @@ EXPORTED = [
     "invdft_adjoint_precondition_jacobi_sqrt", "invdft_adjoint_distribute_x", "invdft_adjoint_solve",
     "invdft_bfgs_solve", "invdft_coldot_noalloc", "invdft_project_vxc_to_parent", "invdft_evaluate_parent_field",
     "invdft_force_backward_at", "invdft_dot_blocks", "invdft_get_index_map",
+    "invdft_poisson_total_potential", "invdft_kernel_probe", "invdft_bfgs_run", "invdft_initial_guess",
 ]
 
 # invdft_get_index_map selectors (include/invdft_force.h)
@@ -71,7 +72,7 @@ class Params(C.Structure):
         ("adjoint_max_iter", C.c_int32), ("degeneracy_tol", C.c_double), ("frac_occ_tol", C.c_double),
         ("additional_states", C.c_int32), ("block_size", C.c_int32), ("inter_block_size", C.c_int32),
         ("factor_lda", C.c_double), ("lanczos_steps", C.c_int32), ("precision", C.c_int32),
-        ("mixed_residual_floor", C.c_double),
+        ("mixed_residual_floor", C.c_double), ("mixed_inner_tol", C.c_double), ("mixed_max_refine", C.c_int32),
     ]
 
 
@@ -86,11 +87,29 @@ class Stats(C.Structure):
         ("n_cell_gemm", C.c_int32), ("ms_cell_gemm", C.c_double), ("cell_gemm_bytes", C.c_double),
         ("cell_gemm_flops", C.c_double), ("n_launches", C.c_int64), ("degree", C.c_int32),
         ("upper_bound", C.c_double), ("device_bytes", C.c_double), ("device_bytes_peak", C.c_double),
-        ("passes_low", C.c_int32), ("generation", C.c_int64),
+        ("passes_low", C.c_int32), ("generation", C.c_int64), ("refine_steps", C.c_int32),
     ]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class BfgsOptions(C.Structure):
+    _fields_ = [("max_iter", C.c_int32), ("tol", C.c_double), ("line_search_iters", C.c_int32),
+                ("line_search_tol", C.c_double), ("history", C.c_int32), ("density_l1_target", C.c_double)]
+
+
+class BfgsReport(C.Structure):
+    _fields_ = [("n_iters", C.c_int32), ("n_evals", C.c_int32), ("final_loss", C.c_double),
+                ("final_density_l1", C.c_double), ("reached", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class InitialGuessOptions(C.Structure):
+    _fields_ = [("tau_vx", C.c_double), ("tau_fa", C.c_double), ("fermi_amaldi_bc", C.c_int32),
+                ("factor_fa", C.c_double), ("hartree_rel_tol", C.c_double), ("hartree_max_iter", C.c_int32)]
 
 
 _lib = None
@@ -124,6 +143,12 @@ def load() -> C.CDLL:
         "invdft_force_backward_at": (C.c_int, [vp, C.c_int64, _f64p, _P(Stats)]),
         "invdft_dot_blocks": (C.c_int, [vp, _f64p, _f64p, C.c_int64, C.c_int32, _f64p]),
         "invdft_get_index_map": (C.c_int, [vp, C.c_int32, _P(C.c_int32), C.c_int64]),
+        "invdft_kernel_probe": (C.c_int, [vp]),
+        "invdft_initial_guess": (C.c_int, [vp, _f64p, _f64p, _f64p, _P(InitialGuessOptions), _f64p, _f64p, _f64p]),
+        "invdft_bfgs_run": (C.c_int, [vp, _f64p, _P(BfgsOptions), _f64p, _f64p, C.c_int32, _P(BfgsReport)]),
+        "invdft_poisson_total_potential": (C.c_int, [vp, _f64p, C.c_int32, _f64p, _i64p, _f64p, C.c_double,
+                                                     C.c_int32, C.c_int32, _f64p, _f64p, _P(C.c_int32),
+                                                     _f64p]),
         "invdft_set_potential": (C.c_int, [vp, _f64p]),
         "invdft_hx": (C.c_int, [vp, vp, vp, C.c_int32]),
         "invdft_project_vxc_to_parent": (C.c_int, [vp, _f64p, _f64p]),

@@ -139,6 +139,43 @@ class InverseDFTSolverFunction:
         _check(self.lib, self.ctx, self.lib.invdft_get_child_quad_products(self.ctx, ptr(out)))
         return out
 
+    def poisson_total_potential(self, rho_quad, Z=(), atom_cell=(), atom_xi=(), rel_tol: float = 1e-12,
+                                max_iter: int = 20000, install: bool = False):
+        """setPotBasePoissonNuclear (InverseDFTEngine.cpp:2459-2571) on the GPU:
+        phi of -lap phi = 4 pi (rho - sum Z delta) with zero boundary values;
+        returns (phi at the parent quadrature points, nodal phi, CG iterations,
+        relative residual).  install=True makes it the base potential."""
+        rho = f64(rho_quad)
+        Zs = f64(np.asarray(Z, dtype=np.float64).reshape(-1))
+        cells = i64(np.asarray(atom_cell, dtype=np.int64).reshape(-1))
+        xi = f64(np.asarray(atom_xi, dtype=np.float64).reshape(-1, 3) if len(Zs) else np.zeros((0, 3)))
+        phi_q = np.zeros(self.problem.n_cells * self.problem.nq)
+        phi_n = np.zeros(self.problem.n_nodes)
+        it = C.c_int32()
+        res = C.c_double()
+        _check(self.lib, self.ctx, self.lib.invdft_poisson_total_potential(
+            self.ctx, ptr(rho), int(Zs.size), ptr(Zs), ptr(cells), ptr(xi), float(rel_tol), int(max_iter),
+            int(bool(install)), ptr(phi_q), ptr(phi_n), C.byref(it), C.byref(res)))
+        return phi_q, phi_n, it.value, res.value
+
+    def initial_guess(self, rho_quad, sigma_quad=None, hartree_bc=None, tau_vx: float = 1e-2,
+                      tau_fa: float = 1e-2, fermi_amaldi_bc: bool = False, factor_fa: float = 1.0,
+                      hartree_rel_tol: float = 1e-12, hartree_max_iter: int = 20000):
+        """setInitialPotL2Proj (InverseDFTEngine.cpp:1046-1498) on the GPU:
+        returns (v_xc guess on the child nodes, parent nodal field, v_H at the
+        parent quadrature points)."""
+        o = native.InitialGuessOptions(tau_vx, tau_fa, int(bool(fermi_amaldi_bc)), factor_fa, hartree_rel_tol,
+                                       hartree_max_iter)
+        rho = f64(rho_quad)
+        sig = None if sigma_quad is None else ptr(f64(sigma_quad))
+        bc = None if hartree_bc is None else ptr(f64(hartree_bc))
+        child = np.zeros(self.problem.n_child_nodes)
+        parent = np.zeros(self.problem.n_nodes)
+        vh = np.zeros(self.problem.n_cells * self.problem.nq)
+        _check(self.lib, self.ctx, self.lib.invdft_initial_guess(self.ctx, ptr(rho), sig, bc, C.byref(o), ptr(child),
+                                                                  ptr(parent), ptr(vh)))
+        return child, parent, vh
+
     def index_map(self, name: str, n: int) -> np.ndarray:
         """An integer index map the library built on the device (int32),
         see invdft_get_index_map."""
@@ -189,6 +226,22 @@ class InverseDFTSolverFunction:
                                                                line_search_iters, line_search_tol, history,
                                                                ptr(losses), C.byref(n)))
         return pot, losses[:n.value]
+
+
+def bfgs_run(fn: "InverseDFTSolverFunction", pot, max_iter: int, density_l1_target: float = 0.0,
+             tol: float = 1e-12, line_search_iters: int = 1, line_search_tol: float = 1e-6, history: int = 100):
+    """L-BFGS (BFGSInverseDFTSolver::solve with the CP line search) that also
+    stops once int |rho - rho*| <= density_l1_target.  Returns (v_xc, report,
+    losses per evaluation, int |rho - rho*| per evaluation)."""
+    pot = f64(pot).copy()
+    o = native.BfgsOptions(max_iter, tol, line_search_iters, line_search_tol, history, density_l1_target)
+    cap = 2 * max_iter + 1
+    losses, l1 = np.zeros(cap), np.zeros(cap)
+    rep = native.BfgsReport()
+    _check(fn.lib, fn.ctx, fn.lib.invdft_bfgs_run(fn.ctx, ptr(pot), C.byref(o), ptr(losses), ptr(l1), cap,
+                                                   C.byref(rep)))
+    n = rep.n_evals
+    return pot, rep.as_dict(), losses[:n], l1[:n]
 
 
 class MultiVectorAdjointLinearSolverProblem:

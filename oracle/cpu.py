@@ -23,7 +23,7 @@ DEFAULTS = dict(cheb_degree=50, max_cheb_passes=100, cheby_tol=1e-6, initial_tol
                 adaptive_factor_cheb=100.0, adjoint_initial_tol=1e-11, adaptive_factor_adjoint=1000.0,
                 adjoint_max_iter=5000, degeneracy_tol=0.002, frac_occ_tol=1e-8, additional_states=0,
                 block_size=0, inter_block_size=10, factor_lda=0.0, lanczos_steps=20, precision=0,
-                mixed_residual_floor=1e-4)
+                mixed_residual_floor=1e-4, mixed_inner_tol=1e-4, mixed_max_refine=12)
 
 
 def load():

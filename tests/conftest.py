@@ -22,7 +22,8 @@ def problem(name: str):
 
 def oracle_params(**kw):
     from oracle import ForceParams
-    kw = {k: v for k, v in kw.items() if k not in ("precision", "mixed_residual_floor")}
+    kw = {k: v for k, v in kw.items()
+          if k not in ("precision", "mixed_residual_floor", "mixed_inner_tol", "mixed_max_refine")}
     base = dict(cheb_degree=30, cheby_tol=1e-10, initial_tol_cheb=1e-10, adjoint_initial_tol=1e-10,
                 adaptive_factor_adjoint=1.0,
                 adjoint_max_iter=2000, max_cheb_passes=60, lanczos_steps=20)

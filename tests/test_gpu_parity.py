@@ -259,6 +259,7 @@ def test_mixed_precision_ladder_reaches_fp64_accuracy(name, variant, monkeypatch
     f_g, L_g, st = fn.get_force_vector(pot.copy())
     f_o, L_o, ost = orc.get_force_vector(pot.copy())
     assert st["passes_low"] >= 1
+    assert st["refine_steps"] >= 2          # FP32-operator MINRES inside FP64 refinement
     assert st["max_residual"] <= 1e-10
     e, _, _ = fn.eigen()
     assert np.max(np.abs(e - ost.eigenvalues)) < 1e-9
@@ -305,3 +306,34 @@ def test_dot_product_blocks_matches_oracle():
     a, b = rng.standard_normal(3001), rng.standard_normal(3001)
     for bs in (1, 3):
         assert fn.dotProduct(a, b, bs) == Oracle.dot_product_blocks(a, b, bs)
+
+
+def test_kernel_probe_leaves_a_usable_context():
+    """The profiling probe launches every kernel once; afterwards the context
+    still evaluates forces equal to the oracle's."""
+    P, fn, orc = _pair("small_lih")
+    fn.set_potential(P.vxc_init.copy())
+    assert fn.lib.invdft_kernel_probe(fn.ctx) == 0
+    f_g, L_g, _ = fn.get_force_vector(P.vxc_init.copy())
+    f_o, L_o, _ = orc.get_force_vector(P.vxc_init.copy())
+    assert rel(f_g, f_o) < TOL_FORCE
+
+
+def test_bfgs_run_stops_at_the_density_target():
+    """invdft_bfgs_run is invdft_bfgs_solve plus a stop once int |rho - rho*|
+    reaches a target: without a target it follows the same iterates, with one
+    it stops at the first accepted iterate below it."""
+    from invdft_b200.solver import bfgs_run
+    P, fn, _ = _pair("tiny_h2")
+    x0 = P.vxc_init.copy()
+    xa, losses = fn.bfgs_solve(x0.copy(), max_iter=3)
+    fn.close()
+    P, fn, _ = _pair("tiny_h2")
+    xb, rep, losses_b, l1 = bfgs_run(fn, x0.copy(), 3)
+    assert np.array_equal(xa, xb) and np.array_equal(losses, losses_b)
+    assert rep["reached"] == 0 and rep["n_iters"] == 3
+    target = 0.5 * (l1[0] + l1[-1])
+    fn.close()
+    P, fn, _ = _pair("tiny_h2")
+    xc, rep, _, l1c = bfgs_run(fn, x0.copy(), 30, density_l1_target=target)
+    assert rep["reached"] == 1 and rep["final_density_l1"] <= target and rep["n_iters"] <= 3

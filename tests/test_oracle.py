@@ -171,3 +171,18 @@ def test_golden_fixture(name):
     assert np.max(np.abs(st.eigenvalues - g["eigenvalues"])) < 1e-10
     assert abs(L - float(g["loss"])) < 1e-10 * abs(float(g["loss"]))
     assert rel(f, g["force"]) < 1e-9
+
+
+def test_poisson_oracle_known_answer():
+    """The base-potential oracle (setPotBasePoissonNuclear restated) on neutral
+    Gaussian atoms approaches the closed form -sum Z erfc(sqrt(beta) r)/r away
+    from the point nuclei."""
+    from invdft_b200.problem.system import rho_atoms, v_base_atoms
+    from oracle.poisson import locate_atoms, total_potential
+    P = problem("small_lih")
+    cells, xi = locate_atoms(P, P.cfg.pos)
+    phi, phi_q = total_potential(P, rho_atoms(P.cfg, P.quad_xyz), P.cfg.Z, cells, xi)
+    r = np.min([np.linalg.norm(P.quad_xyz - np.asarray(a), axis=1) for a in P.cfg.pos], axis=0)
+    far = r > 2.0
+    assert np.max(np.abs(phi_q[far] - v_base_atoms(P.cfg, P.quad_xyz)[far])) < 2e-2
+    assert np.all(phi[P.cons_psi.nodes[np.diff(P.cons_psi.ptr) == 0]] == 0.0)

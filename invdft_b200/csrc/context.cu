@@ -1315,6 +1315,11 @@ void Context::minres_core(const double *d_rhs, double *d_x, double tol, int maxi
   INVDFT_CUDA(cudaMemsetAsync(m_w2.p, 0, v * sizeof(double), stream));
   std::vector<int> act(64);
   const int check_every = 8;
+  bool need_v = true;
+  if (!m_ticket.p) {
+    m_ticket.alloc(1);
+    m_ticket.zero(stream);
+  }
   for (int itn = 1; itn <= maxit; ++itn) {
     if ((itn - 1) % check_every == 0) {
       INVDFT_CUDA(cudaMemcpyAsync(act.data(), st.active, sizeof(int) * Bc, cudaMemcpyDeviceToHost, stream));
@@ -1323,9 +1328,13 @@ void Context::minres_core(const double *d_rhs, double *d_x, double tol, int maxi
       for (int k = 0; k < Bc; ++k)
         if (act[k]) keep.push_back(k);
       if (keep.empty()) break;
-      if ((int)keep.size() < Bc && (4 * (int)keep.size() <= 3 * Bc || (int)keep.size() + 2 <= Bc)) compact(keep);
+      if ((int)keep.size() < Bc && (4 * (int)keep.size() <= 3 * Bc || (int)keep.size() + 2 <= Bc)) {
+        compact(keep);
+        need_v = true;   // v is not part of the re-packed state
+      }
     }
-    launch_minres_v(m_y.p, st, m_v.p, nn, Bc, stream);
+    if (need_v) launch_minres_v(m_y.p, st, m_v.p, nn, Bc, stream);   // else left by the fused update2
+    need_v = false;
     cell_gemm(m_v.p, Bc, low && hx_variant == 3);
     AsmEpilogue epi;
     epi.kind = AsmEpilogue::MINRES;
@@ -1338,9 +1347,9 @@ void Context::minres_core(const double *d_rhs, double *d_x, double tol, int maxi
     launch_reduce_partials(partial.p, nparts, Bc, st.alfa, stream);
     n_hx++;
     n_hx_cols += Bc;
-    launch_minres_update1(m_r1.p, m_r2.p, m_y.p, m_yn.p, diagA.p, st, nn, Bc, partial.p, nblocks_red, stream);
-    launch_minres_scalars(st, Bc, itn, stream);
-    launch_minres_update2(m_xc.p, m_w.p, m_w2.p, m_v.p, st, nn, Bc, stream);
+    launch_minres_update1_fused(m_r1.p, m_r2.p, m_y.p, m_yn.p, diagA.p, st, nn, Bc, partial.p, nblocks_red,
+                                m_ticket.p, stream);
+    launch_minres_update2v(m_xc.p, m_w.p, m_w2.p, m_v.p, m_y.p, st, nn, Bc, stream);
   }
   scatter_x();
   std::vector<int> it_now(Bc);

@@ -119,6 +119,7 @@ class Context {
   DevBuf<double> m_r1, m_r2, m_y, m_v, m_w, m_w2, m_yn, m_b, m_x, m_p, m_xc, m_tmp;
   DevBuf<double> m_scal;           // 16 * maxB doubles
   DevBuf<int> m_flags;             // 3 * maxB ints
+  DevBuf<unsigned> m_ticket;       // CTA ticket of the fused MINRES update (0 between launches)
   std::vector<int> last_iters;
 
   // ---- operations ----

@@ -1464,9 +1464,96 @@ __global__ void __launch_bounds__(NT) minres_update1_kernel(double *__restrict__
   }
 }
 
+// One column's Paige-Saunders scalar update of an iteration (beta2 = the new
+// |r2|_D^2 and alfa already reduced); shared by the scalar kernel and the
+// fused update below.
+__device__ __forceinline__ void minres_column_scalars(const MinresState &st, int b);
+
 __global__ void minres_scalars_kernel(MinresState st, int B) {
   const int b = threadIdx.x;
   if (b >= B) return;
+  minres_column_scalars(st, b);
+}
+
+// update1 with the reduction of its dot partials and the scalar update fused
+// in: the last CTA to finish (a ticket taken after a fence) sums the partials
+// of all CTAs -- one warp per column, lanes over the CTAs in a fixed order --
+// into beta2 and runs the scalars; it then resets the ticket.  The sum order
+// does not depend on which CTA is last, so results are reproducible.
+__global__ void __launch_bounds__(NT) minres_update1_fused_kernel(double *__restrict__ r1, double *__restrict__ r2,
+                                                                  double *__restrict__ y,
+                                                                  const double *__restrict__ yn,
+                                                                  const double *__restrict__ diagA, MinresState st,
+                                                                  int64_t n, int B, int64_t rows_per_block,
+                                                                  double *__restrict__ partial,
+                                                                  unsigned *__restrict__ ticket) {
+  __shared__ double red[NT];
+  __shared__ bool last;
+  const int RR = NT / B;
+  const int j = threadIdx.x % B, rr = threadIdx.x / B;
+  const int64_t r0 = blockIdx.x * rows_per_block;
+  const int64_t r1e = min(n, r0 + rows_per_block);
+  double acc = 0.0;
+  if (rr < RR && st.active[j]) {
+    const double a = st.alfa[j] / st.beta[j];
+    for (int64_t r = r0 + rr; r < r1e; r += RR) {
+      const int64_t idx = r * B + j;
+      const double r2o = r2[idx];
+      const double ynv = yn[idx] - a * r2o;
+      const double yv = diagA[r] * ynv;
+      r1[idx] = r2o;
+      r2[idx] = ynv;
+      y[idx] = yv;
+      acc = fma(ynv, yv, acc);
+    }
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x < B) {
+    double sum = 0.0;
+    for (int q = 0; q < RR; ++q) sum += red[q * B + threadIdx.x];
+    partial[(int64_t)blockIdx.x * B + threadIdx.x] = sum;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int c = warp; c < B; c += NT / 32) {
+    double v = 0.0;
+    for (int g = lane; g < (int)gridDim.x; g += 32) v += __ldcg(&partial[(int64_t)g * B + c]);
+    v = warp_sum(v);
+    if (lane == 0) st.beta2[c] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < B) minres_column_scalars(st, threadIdx.x);
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// update2 (w, w2, x of the committed columns) fused with the next iteration's
+// v = y / beta (beta already the new one): each element is read and written by
+// one thread, so v is updated in place after its old value is used.
+__global__ void minres_update2v_kernel(double *__restrict__ x, double *__restrict__ w, double *__restrict__ w2,
+                                       double *__restrict__ v, const double *__restrict__ y, MinresState st,
+                                       int64_t n, int B) {
+  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= n * B) return;
+  const int b = (int)(idx % B);
+  const double vo = v[idx];
+  if (st.commit[b]) {
+    const double wo = w[idx], w2o = w2[idx];
+    const double wn = (vo - st.oldeps[b] * w2o - st.delta[b] * wo) * st.denom[b];
+    w2[idx] = wo;
+    w[idx] = wn;
+    x[idx] = fma(st.phi[b], wn, x[idx]);
+  }
+  const double bt = st.beta[b];
+  v[idx] = bt > 0.0 ? y[idx] / bt : 0.0;
+}
+
+__device__ __forceinline__ void minres_column_scalars(const MinresState &st, int b) {
   if (!st.active[b]) {
     st.commit[b] = 0;
     return;
@@ -1786,6 +1873,63 @@ __global__ void __launch_bounds__(NT) group_gather_kernel(FeView fe, const doubl
   }
 }
 
+// Narrow blocks (B <= 8: the tail of the MINRES iterations, small meshes): one warp per
+// constraint group instead of a CTA, eight groups per CTA, so the launch fits
+// in one wave and a group's few rows do not idle a whole CTA.  The sums run in
+// the same order as the CTA-per-group kernels, so results are bitwise equal.
+constexpr int kWarpGroupMaxB = 8;
+constexpr int kWarpStageM = 64;   // masters staged per warp (larger groups read global memory)
+
+__global__ void __launch_bounds__(NT) group_gather_warp_kernel(FeView fe, const double *__restrict__ x, int B) {
+  __shared__ double xs[NT / 32][kWarpStageM * kWarpGroupMaxB];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = blockIdx.x * (NT / 32) + warp;
+  if (g >= fe.ngroup) return;   // the whole warp leaves; only warp-level syncs below
+  const int nm = fe.g_nm[g], m0 = fe.g_m0[g];
+  const int rp0 = fe.g_rptr[g], nr = fe.g_rptr[g + 1] - rp0;
+  const double *gw = fe.g_gw + fe.g_woff[g];
+  double *xm = xs[warp];
+  const bool staged = nm <= kWarpStageM && nm * B <= fe.g_stage;
+  if (staged)
+    for (int i = lane; i < nm * B; i += 32) {
+      const int t = i / B, j = i - t * B;
+      xm[i] = x[(int64_t)fe.cons_masters[m0 + t] * B + j];
+    }
+  __syncwarp();
+  for (int i = lane; i < nr * B; i += 32) {
+    const int q = i / B, j = i - q * B;
+    double v = 0.0;
+    for (int t = 0; t < nm; ++t)
+      v = fma(gw[q * nm + t], staged ? xm[t * B + j] : x[(int64_t)fe.cons_masters[m0 + t] * B + j], v);
+    fe.hvg[(int64_t)fe.g_rows[rp0 + q] * B + j] = v;
+  }
+}
+
+__global__ void __launch_bounds__(NT) group_partial_warp_kernel(FeView fe, int B) {
+  __shared__ double zs[NT / 32][kGroupRows * kWarpGroupMaxB];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = blockIdx.x * (NT / 32) + warp;
+  if (g >= fe.ngroup_h) return;
+  const int nm = fe.g_nm[g], rp0 = fe.g_rptr[g], nr = fe.g_rptr[g + 1] - rp0;
+  const int64_t po = fe.g_poff[g];
+  const double *w = fe.g_w + fe.g_woff[g];
+  double *zr = zs[warp];
+  const bool staged = nr * B <= fe.g_stage;
+  if (staged)
+    for (int i = lane; i < nr * B; i += 32) {
+      const int q = i / B, j = i - q * B;
+      zr[i] = fe.z[(int64_t)fe.g_hrow[rp0 + q] * B + j];
+    }
+  __syncwarp();
+  for (int i = lane; i < nm * B; i += 32) {
+    const int t = i / B, j = i - t * B;
+    double acc = 0.0;
+    for (int q = 0; q < nr; ++q)
+      acc = fma(w[q * nm + t], staged ? zr[q * B + j] : fe.z[(int64_t)fe.g_hrow[rp0 + q] * B + j], acc);
+    fe.gpart[(po + t) * B + j] = acc;
+  }
+}
+
 template <int N, int MINB, bool GXS = false, typename T = double>
 static void hx_sf_n(const FeView &fe, const SfMatsT<T> &mt, const double *vj, const double *x, double *Ycell, int B,
                     int mode, cudaStream_t s) {
@@ -1822,6 +1966,11 @@ static void hx_sf_dispatch(const FeView &fe, const SfMats &mt, const double *vj,
 }
 
 static void launch_group_gather(const FeView &fe, const double *x, int B, int gather_mode, cudaStream_t s) {
+  if (gather_mode != GATHER_PLAIN && fe.ngroup > 0 && B <= kWarpGroupMaxB) {
+    group_gather_warp_kernel<<<ceil_div(fe.ngroup, NT / 32), NT, 0, s>>>(fe, x, B);
+    INVDFT_LAUNCH_CHECK();
+    return;
+  }
   if (gather_mode != GATHER_PLAIN && fe.ngroup > 0) {
     // staging capacity: the largest group's need, at most fe.g_stage doubles
     const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnm, 1) * (B + fe.g_maxnr), fe.g_stage);
@@ -2013,7 +2162,12 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
     hanging_sum_kernel<<<ceil_div((int64_t)fe.nhang * B, NT), NT, 0, s>>>(fe, Ycell, B);
     INVDFT_LAUNCH_CHECK();
   }
-  if (fe.nmast > 0) {
+  if (fe.nmast > 0 && B <= kWarpGroupMaxB) {
+    group_partial_warp_kernel<<<ceil_div(fe.ngroup_h, NT / 32), NT, 0, s>>>(fe, B);
+    INVDFT_LAUNCH_CHECK();
+    master_sum_kernel<<<ceil_div((int64_t)fe.nmast * B, NT), NT, 0, s>>>(fe, B);
+    INVDFT_LAUNCH_CHECK();
+  } else if (fe.nmast > 0) {
     const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnr, 1) * (B + std::max(fe.g_maxnm, 1)),
                                            fe.g_stage);
     static bool attr = false;
@@ -2192,6 +2346,20 @@ void launch_minres_update1(double *r1, double *r2, double *y, const double *yn, 
   minres_update1_kernel<<<nblocks, NT, 0, s>>>(r1, r2, y, yn, diagA, st, n, B, rpb, partial);
   INVDFT_LAUNCH_CHECK();
   launch_reduce_partials(partial, nblocks, B, st.beta2, s);
+}
+
+void launch_minres_update1_fused(double *r1, double *r2, double *y, const double *yn, const double *diagA,
+                                 const MinresState &st, int64_t n, int B, double *partial, int nblocks,
+                                 unsigned *ticket, cudaStream_t s) {
+  const int64_t rpb = (n + nblocks - 1) / nblocks;
+  minres_update1_fused_kernel<<<nblocks, NT, 0, s>>>(r1, r2, y, yn, diagA, st, n, B, rpb, partial, ticket);
+  INVDFT_LAUNCH_CHECK();
+}
+
+void launch_minres_update2v(double *x, double *w, double *w2, double *v, const double *y, const MinresState &st,
+                            int64_t n, int B, cudaStream_t s) {
+  minres_update2v_kernel<<<ceil_div(n * B, NT), NT, 0, s>>>(x, w, w2, v, y, st, n, B);
+  INVDFT_LAUNCH_CHECK();
 }
 
 void launch_minres_scalars(const MinresState &st, int B, int itn, cudaStream_t s) {

@@ -199,6 +199,14 @@ void launch_minres_update2(double *x, double *w, double *w2, const double *v, co
 void launch_minres_init(const double *b, const double *diagA, double *r1, double *r2, double *y,
                         int64_t n, int B, double *partial, int nblocks, cudaStream_t s);
 void launch_minres_init_scalars(const MinresState &st, const double *beta1_sq, int B, cudaStream_t s);
+// update1 + the reduction of beta2 + the scalar update in one launch (the last
+// CTA reduces and updates; *ticket must be 0 before, and is 0 after)
+void launch_minres_update1_fused(double *r1, double *r2, double *y, const double *yn, const double *diagA,
+                                 const MinresState &st, int64_t n, int B, double *partial, int nblocks,
+                                 unsigned *ticket, cudaStream_t s);
+// update2 + the next iteration's v = y / beta in one launch (v in place)
+void launch_minres_update2v(double *x, double *w, double *w2, double *v, const double *y, const MinresState &st,
+                            int64_t n, int B, cudaStream_t s);
 
 // Child mesh transfers
 struct ChildView {

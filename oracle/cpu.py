@@ -50,6 +50,7 @@ def load():
         "ocpu_get_psi": (C.c_int, [vp, f64p]),
         "ocpu_density": (C.c_int, [vp, f64p]),
         "ocpu_set_state": (C.c_int, [vp, f64p, f64p, C.c_int, C.c_double, C.c_double, C.c_double]),
+        "ocpu_lanczos_bounds": (C.c_int, [vp, C.c_int, f64p, f64p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -123,6 +124,12 @@ class CpuForce:
 
     def set_potential(self, pot):
         self._check(self.lib.ocpu_set_potential(self.ctx, ptr(f64(pot))))
+
+    def lanczos_bounds(self, steps: int):
+        """(lower, upper) spectrum bounds of a `steps`-step Lanczos run at the current potential."""
+        lo, hi = C.c_double(), C.c_double()
+        self._check(self.lib.ocpu_lanczos_bounds(self.ctx, int(steps), C.byref(lo), C.byref(hi)))
+        return lo.value, hi.value
 
     def hx(self, x):
         x = f64(x)

@@ -1404,6 +1404,19 @@ int ocpu_set_state(void *ctx, const double *psi, const double *eig, int counter,
   });
 }
 
+// the spectrum bounds of solveEigen's Lanczos run with `steps` steps at the
+// current potential (set_potential first)
+int ocpu_lanczos_bounds(void *ctx, int steps, double *lo, double *hi) {
+  return ocpu_guard([&] {
+    ocpu::Ctx &c = *static_cast<ocpu::Ctx *>(ctx);
+    if (c.vj.empty()) throw ocpu::Error(INVDFT_NOT_READY, "no potential set");
+    const int keep = c.prm.lanczos_steps;
+    c.prm.lanczos_steps = steps;
+    ocpu::Eigen(c).bounds(*lo, *hi);
+    c.prm.lanczos_steps = keep;
+  });
+}
+
 int ocpu_set_potential(void *ctx, const double *pot) {
   return ocpu_guard([&] {
     ocpu::Ctx &c = *static_cast<ocpu::Ctx *>(ctx);

@@ -497,6 +497,12 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
     // autotuned on its first use (sf_shape)
     const char *t = std::getenv("INVDFT_SF_TUNE");
     sf_tune = t ? std::atoi(t) : -1;
+    // INVDFT_MINRES_FUSED=0: the MINRES update as separate launches
+    const char *mf = std::getenv("INVDFT_MINRES_FUSED");
+    minres_fused = !(mf && std::string(mf) == "0");
+    // INVDFT_TRACE=1: one line per Chebyshev pass on stderr (diagnostics)
+    const char *tr = std::getenv("INVDFT_TRACE");
+    trace = tr && std::string(tr) == "1";
     for (int &v : sf_tuned) v = -1;
   }
   fe.inv_sqrt_mass = invsqrtM.p; fe.sqrt_mass = sqrtM.p;
@@ -598,6 +604,7 @@ int Context::sf_shape(const double *d_x, int Bw) {
   std::vector<int> cand = {0};
   if (n1 <= 6) cand.push_back(1);
   if (n1 == 6) cand.push_back(2);
+  if (n1 == 5 || n1 == 6) cand.push_back(3);
   if (cand.size() == 1) return t = 0;
   cudaEvent_t a, b;
   INVDFT_CUDA(cudaEventCreate(&a));
@@ -953,6 +960,10 @@ void Context::solve_eigen(double *d_pot, invdft_force_stats *st) {
       if (occ[i] > prm.frac_occ_tol || i <= homo + prm.additional_states) maxres = std::max(maxres, res[i]);
     ++passes;
     if (low) ++passes_low;
+    if (trace)
+      std::fprintf(stderr, "chebyshev pass %d%s: max residual %.3e (tol %.1e), filter [%.6g, %.6g] a0 %.6g, "
+                   "mu %.6g, eig[0] %.6g eig[N-1] %.6g, homo %d\n", passes, low ? " (FP32)" : "", maxres, tol_cheb,
+                   a, b, a0, mu, eig.front(), eig.back(), homo);
     if (!(maxres > tol_cheb && passes < prm.max_cheb_passes)) break;
     if (low && (maxres < prm.mixed_residual_floor || maxres > 0.5 * prev_maxres)) low = false;
     prev_maxres = maxres;
@@ -1347,9 +1358,16 @@ void Context::minres_core(const double *d_rhs, double *d_x, double tol, int maxi
     launch_reduce_partials(partial.p, nparts, Bc, st.alfa, stream);
     n_hx++;
     n_hx_cols += Bc;
-    launch_minres_update1_fused(m_r1.p, m_r2.p, m_y.p, m_yn.p, diagA.p, st, nn, Bc, partial.p, nblocks_red,
-                                m_ticket.p, stream);
-    launch_minres_update2v(m_xc.p, m_w.p, m_w2.p, m_v.p, m_y.p, st, nn, Bc, stream);
+    if (minres_fused) {
+      launch_minres_update1_fused(m_r1.p, m_r2.p, m_y.p, m_yn.p, diagA.p, st, nn, Bc, partial.p, nblocks_red,
+                                  m_ticket.p, stream);
+      launch_minres_update2v(m_xc.p, m_w.p, m_w2.p, m_v.p, m_y.p, st, nn, Bc, stream);
+    } else {
+      launch_minres_update1(m_r1.p, m_r2.p, m_y.p, m_yn.p, diagA.p, st, nn, Bc, partial.p, nblocks_red, stream);
+      launch_minres_scalars(st, Bc, itn, stream);
+      launch_minres_update2(m_xc.p, m_w.p, m_w2.p, m_v.p, st, nn, Bc, stream);
+      need_v = true;
+    }
   }
   scatter_x();
   std::vector<int> it_now(Bc);

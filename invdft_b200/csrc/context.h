@@ -54,6 +54,8 @@ class Context {
   // on stored cell matrices (mma.sync f64), 1 row-stream DFMA, 2 bulk-staged DFMA
   int hx_variant = 3;
   int sf_tune = -1;                // launch shape of the matrix-free kernel (-1: autotuned per width)
+  bool minres_fused = true;        // MINRES update1 + reductions + scalars, update2 + v, in two launches
+  bool trace = false;              // per-pass lines of the eigensolver on stderr
   int sf_tuned[65];                // autotuned shape per block width (-1: not measured yet)
   int sf_shape(const double *d_x, int Bw);
   SfMats sfm{};                    // reference-element matrices of the matrix-free variant

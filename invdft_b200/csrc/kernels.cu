@@ -427,7 +427,20 @@ __device__ __forceinline__ void sf_phit(const SfMatsT<T> &mt, const T (&in)[N], 
   }
 }
 
-template <int N, int MINB, bool GXS, typename T = double>
+// Asynchronous 8- and 4-byte global -> shared copies (cp.async, zero-filled
+// when `valid` is false), completed by cp_async_wait_all in the same thread.
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(sa), "l"(gmem), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(sa), "l"(gmem), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <int N, int MINB, bool GXS, typename T = double, bool PRE = false>
 __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe, SfMatsT<T> mt, const double *__restrict__ vj,
                                                                 const double *__restrict__ x,
                                                                 double *__restrict__ Ycell, int B, int C, int mode) {
@@ -435,17 +448,27 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
   // of registers between the forward and the backward x pass.  T is the
   // arithmetic type (double; float for the low rungs of the precision ladder):
   // the gathered values and v JxW are rounded to T, the results widened to
-  // double in the cell-result slots.
+  // double in the cell-result slots.  PRE: the potential values and, once
+  // those are used, the slot indices of the thread's z-line are copied into a
+  // further shared array with cp.async at the start, so their global latency
+  // hides behind the first stages instead of stalling the stages that use them.
   constexpr int N2 = N * N, N3 = N2 * N;
   extern __shared__ __align__(16) unsigned char sf_smem[];
   T *sm = reinterpret_cast<T *>(sf_smem);
   T *A = sm, *Bs = sm + N3 * 16, *Cs = sm + 2 * N3 * 16, *Gs = sm + 3 * N3 * 16;
+  double *Vs = reinterpret_cast<double *>(sm + (GXS ? 4 : 3) * N3 * 16);   // PRE: [point][pair]
   const int p = threadIdx.x & 15, L = threadIdx.x >> 4;
   const int G = 16 / C;
   const int g = p / C, c = p - g * C;
   const int64_t e = (int64_t)blockIdx.x * G + g;
   const int b = blockIdx.y * C + c;
   const bool act = e < fe.nc && b < B;
+  if (PRE) {
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+      cp_async8(&Vs[sf_point<N, 2>(L, k) * 16 + p], act ? &vj[e * N3 + L + N2 * k] : vj, act);
+    cp_async_commit();
+  }
   const T hh = act ? T(0.5 * fe.cell_h[e]) : T(0);
   T wa = T(0), wb = T(0);   // weights of the two coordinates off the line (compile-time indices)
 #pragma unroll
@@ -497,8 +520,19 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
   sf_store<N, 1>(Cs, L, p, s);
   {
     T v[N];
+    if (PRE) {
+      cp_async_wait_all();
 #pragma unroll
-    for (int k = 0; k < N; ++k) v[k] = act ? T(vj[e * N3 + L + N2 * k]) : T(0);
+      for (int k = 0; k < N; ++k) v[k] = T(Vs[sf_point<N, 2>(L, k) * 16 + p]);
+      // the slot indices of the output, into the low half of each used entry
+#pragma unroll
+      for (int k = 0; k < N; ++k)
+        cp_async4(&Vs[sf_point<N, 2>(L, k) * 16 + p], act ? &fe.slot_of[e * N3 + L + N2 * k] : fe.slot_of, act);
+      cp_async_commit();
+    } else {
+#pragma unroll
+      for (int k = 0; k < N; ++k) v[k] = act ? T(vj[e * N3 + L + N2 * k]) : T(0);
+    }
     sf_load<N, 2>(A, L, p, r);           // d/dz, the z back pass and the potential term
     sf_dq<N>(mt, r, s);
 #pragma unroll
@@ -527,10 +561,12 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
   __syncthreads();
   sf_load<N, 2>(A, L, p, r);             // phi^T along z, straight to the cell-result slots
   sf_phit<N>(mt, r, s);
+  if (PRE) cp_async_wait_all();
   if (act) {
 #pragma unroll
     for (int k = 0; k < N; ++k) {
-      const int sl = fe.slot_of[e * N3 + L + N2 * k];
+      const int sl = PRE ? *reinterpret_cast<const int *>(&Vs[sf_point<N, 2>(L, k) * 16 + p])
+                         : fe.slot_of[e * N3 + L + N2 * k];
       if (sl >= 0) Ycell[(int64_t)sl * B + b] = double(s[k]);
     }
   }
@@ -1930,15 +1966,15 @@ __global__ void __launch_bounds__(NT) group_partial_warp_kernel(FeView fe, int B
   }
 }
 
-template <int N, int MINB, bool GXS = false, typename T = double>
+template <int N, int MINB, bool GXS = false, typename T = double, bool PRE = false>
 static void hx_sf_n(const FeView &fe, const SfMatsT<T> &mt, const double *vj, const double *x, double *Ycell, int B,
                     int mode, cudaStream_t s) {
   constexpr int threads = 16 * N * N;
-  const size_t smem = sizeof(T) * (GXS ? 4 : 3) * (size_t)N * N * N * 16;
+  const size_t smem = sizeof(T) * (GXS ? 4 : 3) * (size_t)N * N * N * 16 + (PRE ? sizeof(double) * N * N * N * 16 : 0);
   static bool attr = false;
   if (!attr) {
-    INVDFT_CUDA(cudaFuncSetAttribute(hx_cell_sf_kernel<N, MINB, GXS, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_cell_sf_kernel<N, MINB, GXS, T, PRE>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = true;
   }
   // C columns of 16/C cells per CTA; C = the smallest power of two >= B, at most 16
@@ -1946,7 +1982,7 @@ static void hx_sf_n(const FeView &fe, const SfMatsT<T> &mt, const double *vj, co
   while (C < B && C < 16) C <<= 1;
   const int G = 16 / C;
   const dim3 grid((unsigned)((fe.nc + G - 1) / G), (unsigned)((B + C - 1) / C));
-  hx_cell_sf_kernel<N, MINB, GXS, T><<<grid, threads, smem, s>>>(fe, mt, vj, x, Ycell, B, C, mode);
+  hx_cell_sf_kernel<N, MINB, GXS, T, PRE><<<grid, threads, smem, s>>>(fe, mt, vj, x, Ycell, B, C, mode);
   INVDFT_LAUNCH_CHECK();
 }
 
@@ -1965,8 +2001,17 @@ static void hx_sf_dispatch(const FeView &fe, const SfMats &mt, const double *vj,
   }
 }
 
+// INVDFT_GROUP_WARP=0 keeps the CTA-per-group constraint kernels at every width
+static bool group_warp_enabled() {
+  static const bool on = [] {
+    const char *v = std::getenv("INVDFT_GROUP_WARP");
+    return !(v && std::string(v) == "0");
+  }();
+  return on;
+}
+
 static void launch_group_gather(const FeView &fe, const double *x, int B, int gather_mode, cudaStream_t s) {
-  if (gather_mode != GATHER_PLAIN && fe.ngroup > 0 && B <= kWarpGroupMaxB) {
+  if (gather_mode != GATHER_PLAIN && fe.ngroup > 0 && B <= kWarpGroupMaxB && group_warp_enabled()) {
     group_gather_warp_kernel<<<ceil_div(fe.ngroup, NT / 32), NT, 0, s>>>(fe, x, B);
     INVDFT_LAUNCH_CHECK();
     return;
@@ -2004,6 +2049,14 @@ void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, con
   launch_group_gather(fe, x, B, gather_mode, s);
   if (tune == 2 && fe.n1 == 6) {   // two CTAs per SM, derivative lines in shared memory
     hx_sf_n<6, 2, true>(fe, mt, vj, x, Ycell, B, gather_mode, s);
+    return;
+  }
+  if (tune == 3 && fe.n1 == 6) {   // two CTAs per SM, potential and slot indices prefetched by cp.async
+    hx_sf_n<6, 2, false, double, true>(fe, mt, vj, x, Ycell, B, gather_mode, s);
+    return;
+  }
+  if (tune == 3 && fe.n1 == 5) {
+    hx_sf_n<5, 2, false, double, true>(fe, mt, vj, x, Ycell, B, gather_mode, s);
     return;
   }
   if (tune >= 1 && fe.n1 <= 6) {
@@ -2162,7 +2215,7 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
     hanging_sum_kernel<<<ceil_div((int64_t)fe.nhang * B, NT), NT, 0, s>>>(fe, Ycell, B);
     INVDFT_LAUNCH_CHECK();
   }
-  if (fe.nmast > 0 && B <= kWarpGroupMaxB) {
+  if (fe.nmast > 0 && B <= kWarpGroupMaxB && group_warp_enabled()) {
     group_partial_warp_kernel<<<ceil_div(fe.ngroup_h, NT / 32), NT, 0, s>>>(fe, B);
     INVDFT_LAUNCH_CHECK();
     master_sum_kernel<<<ceil_div((int64_t)fe.nmast * B, NT), NT, 0, s>>>(fe, B);

@@ -267,7 +267,7 @@ def test_mixed_precision_ladder_reaches_fp64_accuracy(name, variant, monkeypatch
     assert rel(f_g, f_o) < 1e-6
 
 
-@pytest.mark.parametrize("name", ["small_lih", "tiny_h2_p5"])
+@pytest.mark.parametrize("name", ["small_lih", "tiny_h2_p5", "tiny_h2_p4"])
 def test_sf_launch_shapes_are_bitwise_identical(name, monkeypatch):
     """The matrix-free kernel's launch shapes (one or two CTAs per SM,
     derivative lines in registers or shared memory) run the same FMA sequence,
@@ -279,7 +279,7 @@ def test_sf_launch_shapes_are_bitwise_identical(name, monkeypatch):
     else:
         from invdft_b200.problem.system import build_problem
         P = build_problem(name, target_solver="atoms")
-    shapes = ["0", "1"] + (["2"] if P.p == 5 else [])
+    shapes = ["0", "1"] + (["2"] if P.p == 5 else []) + (["3"] if P.p in (4, 5) else [])
     out = {}
     for shape in shapes + ["auto"]:
         if shape == "auto":

@@ -273,8 +273,13 @@ def aggregate(ms: float, e2e_s: float, steps: int, world: int, dist=None, device
     return steps * world / (ms / 1000.0), steps * world / e2e_s, ms
 
 
+PATH_START = 0.0   # --path-start
+
+
 def trajectory(P, k: int, total: int):
-    a = 0.5 * (k + 1) / max(total, 1)
+    """Point k of total on the straight path guess -> v_xc*: the fraction
+    a = s + (1 - s) (k + 1) / (2 total) of the way, s = --path-start."""
+    a = PATH_START + (1.0 - PATH_START) * 0.5 * (k + 1) / max(total, 1)
     return P.vxc_init + a * (P.vxc_exact - P.vxc_init)
 
 
@@ -350,6 +355,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c1_c2h4")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--ladder-operands", default="fp32", choices=["fp32", "tf32", "bf16"],
+                    help="--precision mixed: operands of the low-rung filter products, rounded as a tensor-core "
+                         "MMA of that input format would round them (FP32 accumulation)")
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="do not time the FP64 path on the same trajectory")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU evaluation (profiling runs)")
@@ -364,7 +372,12 @@ def main():
     ap.add_argument("--hx-width", type=str, default="0",
                     help="kernel probe for profiling: --steps Lowdin HX applications of a seeded block of this "
                          "width at v_xc = the initial guess, timed with CUDA events (no force evaluation)")
+    ap.add_argument("--path-start", type=float, default=0.0,
+                    help="fraction of the way from the initial guess to v_xc* where the evaluated path starts "
+                         "(0: the guess itself)")
     args = ap.parse_args()
+    global PATH_START
+    PATH_START = args.path_start
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -399,7 +412,9 @@ def main():
 
     P, info = build_workload(args.config)
     from invdft_b200.solver import InverseDFTSolverFunction
+    os.environ["INVDFT_LADDER_OPERANDS"] = args.ladder_operands   # read when the context is created
     fn = InverseDFTSolverFunction(P, force_params(args.precision))
+    os.environ["INVDFT_LADDER_OPERANDS"] = "fp32"
     lib = fn.lib
     lib.invdft_set_profiling(fn.ctx, 1)
     total = args.warmup + args.steps
@@ -514,8 +529,9 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "force-evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else ("f64 + f32 (FP32 matrix-free cell products in the early "
-                                                          "Chebyshev passes)" if matrix_free else
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else (
+                f"f64 + f32 (FP32 matrix-free cell products in the early Chebyshev passes, operands "
+                f"{args.ladder_operands}; FP32-operator MINRES in FP64 refinement)" if matrix_free else
                                                           "f64 + f32 (FP32-stored cell matrices in the early "
                                                           "Chebyshev passes)"),
             "data": "synthetic (seeded; see invdft_b200/problem/system.py)",
@@ -530,6 +546,7 @@ def main():
                 "chebyshev_degree": [s["degree"] for s in stats],
                 "spectrum_upper_bound": stats[-1]["upper_bound"],
                 "minres_iters_max": [s["minres_iters_max"] for s in stats],
+                "minres_iters_sum": [s["minres_iters_sum"] for s in stats],
                 "adjoint_refinement_steps": [s["refine_steps"] for s in stats],
                 "hx_columns": [s["n_hx_columns"] for s in stats],
                 "stage_ms_mean": {k: float(np.mean([s[f"ms_{k}"] for s in stats]))

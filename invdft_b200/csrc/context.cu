@@ -125,9 +125,13 @@ void build_scatter(int64_t nrows, int64_t ncell, int per_cell, const int64_t *ce
 // node then by (cell, local); rows of hanging nodes in slots after those,
 // grouped by hanging node (zptr ranges, summed into z[hanging node] first,
 // then carried to the masters by the constraint groups); Dirichlet rows dropped.
+// Each master of hanging nodes (midx[n] >= 0) owns one more slot, the last of
+// its range, which the master-sum pass fills with the node's pre-summed
+// hanging contributions (mslot[midx[n]]), so that the assembly's sum over the
+// node's contiguous slots already includes them.
 void build_slots(int64_t nrows, int64_t ncell, int per_cell, const int64_t *cell_nodes,
-                 const invdft_constraints &c, std::vector<int> &slot_of, std::vector<int> &dptr,
-                 std::vector<int> &zptr) {
+                 const invdft_constraints &c, const std::vector<int> &midx, std::vector<int> &slot_of,
+                 std::vector<int> &dptr, std::vector<int> &zptr, std::vector<int> &mslot) {
   std::vector<int64_t> crow(nrows, -1), hidx(c.n_rows, -1);
   for (int64_t r = 0; r < c.n_rows; ++r) crow[c.rows[r]] = r;
   int64_t nh = 0;
@@ -141,7 +145,14 @@ void build_slots(int64_t nrows, int64_t ncell, int per_cell, const int64_t *cell
     if (r < 0) cnt[n + 1]++;
     else if (hidx[r] >= 0) zcnt[hidx[r] + 1]++;
   }
+  int nmast = 0;
+  for (int64_t n = 0; n < nrows; ++n)
+    if (midx[n] >= 0) {
+      cnt[n + 1]++;
+      nmast = std::max(nmast, midx[n] + 1);
+    }
   for (int64_t n = 0; n < nrows; ++n) cnt[n + 1] += cnt[n];
+  if (cnt[nrows] + (int64_t)tot > INT32_MAX) throw StatusError(INVDFT_BAD_ARG, "more than 2^31 result slots");
   for (int64_t h = 0; h < nh; ++h) zcnt[h + 1] += zcnt[h];
   const int64_t ndirect = cnt[nrows];
   dptr.assign(cnt.begin(), cnt.end());
@@ -154,6 +165,9 @@ void build_slots(int64_t nrows, int64_t ncell, int per_cell, const int64_t *cell
     if (r < 0) slot_of[t] = (int)fill[n]++;
     else if (hidx[r] >= 0) slot_of[t] = (int)(ndirect + zfill[hidx[r]]++);
   }
+  mslot.assign(std::max(nmast, 1), 0);
+  for (int64_t n = 0; n < nrows; ++n)
+    if (midx[n] >= 0) mslot[midx[n]] = (int)(dptr[n + 1] - 1);
 }
 
 // Constraint rows grouped by identical ordered master lists (at most
@@ -327,6 +341,8 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
         }
     }
     sfm32 = sfm.as<float>();
+    sfm_tf32 = sfm.as<Tf32Operand>();
+    sfm_bf16 = sfm.as<Bf16Operand>();
   }
   std::vector<double> w3(nd);
   for (int i = 0; i < nd; ++i) w3[i] = gw[i % n1] * gw[(i / n1) % n1] * gw[i / (n1 * n1)];
@@ -367,9 +383,11 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   const int64_t nmast = d->cons_psi.n_rows ? d->cons_psi.ptr[d->cons_psi.n_rows] : 0;
   std::vector<double> cgw(std::max<int64_t>(nmast, 1), 0.0);
   for (int64_t k = 0; k < nmast; ++k) cgw[k] = d->cons_psi.weights[k] * ism[d->cons_psi.masters[k]];
-  std::vector<int> slot_of, dptr_h, zptr_h;
-  build_slots(nn, nc, nd, d->cell_nodes, d->cons_psi, slot_of, dptr_h, zptr_h);
+  const ConsGroups G = build_groups(nn, d->cons_psi);
+  std::vector<int> slot_of, dptr_h, zptr_h, mslot_h;
+  build_slots(nn, nc, nd, d->cell_nodes, d->cons_psi, G.midx, slot_of, dptr_h, zptr_h, mslot_h);
   nhang = (int)zptr_h.size() - 1;
+  n_slots = zptr_h.back();
 
   phi.upload(ph, s);
   Kref.upload(K, s);
@@ -382,6 +400,28 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   weight.upload(d->weight, nc * nq, s);
   cell_nodes.upload(cn, s);
   cell_map.upload(cm, s);
+  {
+    // the matrix-free kernel's gather map: a constrained entry names its row of
+    // the pre-gathered values, -(1 + compact hanging index), or -(1 + nh) (a
+    // zero row) for a Dirichlet row; row-major, then [nd][nc] for the
+    // narrow-block CTAs, as is the slot map
+    int nh = 0;
+    for (int64_t r = 0; r < d->cons_psi.n_rows; ++r) nh += d->cons_psi.ptr[r + 1] > d->cons_psi.ptr[r];
+    std::vector<int> hrow_of(d->cons_psi.n_rows);
+    for (int64_t r = 0, h = 0; r < d->cons_psi.n_rows; ++r)
+      hrow_of[r] = d->cons_psi.ptr[r + 1] > d->cons_psi.ptr[r] ? (int)h++ : nh;
+    check(nh == nhang, "hanging row count mismatch");
+    std::vector<int> msf(cm.size());
+    for (size_t t = 0; t < cm.size(); ++t) msf[t] = cm[t] >= 0 ? cm[t] : -(1 + hrow_of[-cm[t] - 1]);
+    cell_map_sf.upload(msf, s);
+    std::vector<int> t(cm.size());
+    for (int64_t e = 0; e < nc; ++e)
+      for (int l = 0; l < nd; ++l) t[(size_t)l * nc + e] = msf[(size_t)e * nd + l];
+    cell_map_t.upload(t, s);
+    for (int64_t e = 0; e < nc; ++e)
+      for (int l = 0; l < nd; ++l) t[(size_t)l * nc + e] = slot_of[(size_t)e * nd + l];
+    d_slot_of_t.upload(t, s);
+  }
   upload_cons(cpsi, d->cons_psi, nn, s);
   upload_cons(cadj, d->cons_adj, nn, s);
   upload_cons(cchild, d->cons_child, ncn, s);
@@ -392,9 +432,8 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   dptr_h.resize(dptr_h.size() + 8, dptr_h.back());
   d_dptr.upload(dptr_h, s);
   {
-    const ConsGroups G = build_groups(nn, d->cons_psi);
     n_masters = G.nmast;
-    d_midx.upload(G.midx, s);
+    d_mslot.upload(mslot_h, s);
     d_g_rptr.upload(G.rptr, s);
     d_g_rows.upload(G.rows.empty() ? std::vector<int>{0} : G.rows, s);
     d_g_hrow.upload(G.hrow.empty() ? std::vector<int>{0} : G.hrow, s);
@@ -403,23 +442,37 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
     d_g_poff.upload(G.poff.empty() ? std::vector<int>{0} : G.poff, s);
     d_mp_ptr.upload(G.mp_ptr, s);
     d_mp_idx.upload(G.mp_idx, s);
-    d_mz.alloc((size_t)std::max(G.nmast, 1) * 64);
     d_gpart.alloc((size_t)std::max(G.npairs, 1) * 64);
     {
-      // weights of each group's rows laid out contiguously, [row][master]
-      std::vector<double> gw(std::max<int64_t>(G.nw, 1), 0.0), w(std::max<int64_t>(G.nw, 1), 0.0);
-      for (int g = 0; g < G.ngroup; ++g)
-        for (int q = G.rptr[g]; q < G.rptr[g + 1]; ++q) {
-          const int64_t base = d->cons_psi.ptr[G.rows[q]];
-          const int64_t o = G.woff[g] + (int64_t)(q - G.rptr[g]) * G.nm[g];
-          for (int t = 0; t < G.nm[g]; ++t) {
-            gw[o + t] = cgw[base + t];
-            w[o + t] = d->cons_psi.weights[base + t];
-          }
+      // the plain weights of each group's rows, [row q][master t] (read by the
+      // transpose) and [t][q] (read by the gather), each distinct block stored
+      // once: groups of the same refinement pattern share bit-identical blocks
+      std::vector<double> w, wt;
+      std::map<std::vector<double>, int64_t> seen;
+      std::vector<int64_t> woff(std::max(G.ngroup, 1), 0);
+      for (int g = 0; g < G.ngroup_h; ++g) {
+        const int nr = G.rptr[g + 1] - G.rptr[g], nm = G.nm[g];
+        std::vector<double> blk((size_t)nr * nm);
+        for (int q = 0; q < nr; ++q) {
+          const int64_t base = d->cons_psi.ptr[G.rows[G.rptr[g] + q]];
+          for (int t = 0; t < nm; ++t) blk[(size_t)q * nm + t] = d->cons_psi.weights[base + t];
         }
-      d_g_woff.upload(G.woff.empty() ? std::vector<int64_t>{0} : G.woff, s);
-      d_g_gw.upload(gw, s);
+        std::vector<double> key(blk);
+        key.push_back((double)nr);
+        auto it = seen.find(key);
+        if (it == seen.end()) {
+          it = seen.emplace(std::move(key), (int64_t)w.size()).first;
+          w.insert(w.end(), blk.begin(), blk.end());
+          for (int t = 0; t < nm; ++t)
+            for (int q = 0; q < nr; ++q) wt.push_back(blk[(size_t)q * nm + t]);
+        }
+        woff[g] = it->second;
+      }
+      if (w.empty()) { w.push_back(0.0); wt.push_back(0.0); }
+      n_weight_blocks = (int)seen.size();
+      d_g_woff.upload(woff, s);
       d_g_w.upload(w, s);
+      d_g_wt.upload(wt, s);
     }
     fe.ngroup = G.ngroup; fe.ngroup_h = G.ngroup_h; fe.g_maxnm = G.maxnm; fe.g_maxnr = G.maxnr;
     // INVDFT_GROUP_STAGE (doubles, diagnostics) lowers the shared staging of a
@@ -428,7 +481,6 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
     fe.g_stage = gs ? std::max(0, std::min(std::atoi(gs), kGroupStage)) : kGroupStage;
   }
   d_zptr.upload(zptr_h, s);
-  d_z.alloc((size_t)std::max(nhang, 1) * 64);
   d_err.alloc(1);
   d_err.zero(s);
   sqrtM.upload(sm, s);
@@ -478,13 +530,15 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   fe.cons_ptr = cpsi.ptr.p; fe.cons_masters = cpsi.masters.p; fe.cons_w = cpsi.w.p; fe.cons_gw = cons_gw.p;
   fe.cons_rows = cpsi.rows.p; fe.ncons = cpsi.n;
   fe.slot_of = d_slot_of.p; fe.dptr = d_dptr.p;
-  fe.zptr = d_zptr.p; fe.nhang = nhang; fe.z = d_z.p;
-  fe.midx = d_midx.p; fe.nmast = n_masters; fe.mz = d_mz.p;
+  fe.cell_map_t = cell_map_t.p; fe.slot_of_t = d_slot_of_t.p;
+  fe.zptr = d_zptr.p; fe.nhang = nhang;
+  fe.nmast = n_masters; fe.mslot = d_mslot.p;
   fe.g_rptr = d_g_rptr.p; fe.g_rows = d_g_rows.p; fe.g_hrow = d_g_hrow.p; fe.g_m0 = d_g_m0.p;
   fe.g_nm = d_g_nm.p; fe.g_poff = d_g_poff.p; fe.mp_ptr = d_mp_ptr.p; fe.mp_idx = d_mp_idx.p;
   fe.gpart = d_gpart.p;
-  fe.g_woff = d_g_woff.p; fe.g_gw = d_g_gw.p; fe.g_w = d_g_w.p;
-  d_hvg.alloc((size_t)std::max(cpsi.n, 1) * 64);
+  fe.g_woff = d_g_woff.p; fe.g_w = d_g_w.p; fe.g_wt = d_g_wt.p;
+  fe.cell_map_sf = cell_map_sf.p;
+  d_hvg.alloc((size_t)(nhang + 1) * 64);   // hanging rows, then the zero row of the Dirichlet entries
   fe.hvg = d_hvg.p;
   fe.err = d_err.p;
   {
@@ -503,6 +557,15 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
     // INVDFT_TRACE=1: one line per Chebyshev pass on stderr (diagnostics)
     const char *tr = std::getenv("INVDFT_TRACE");
     trace = tr && std::string(tr) == "1";
+    // INVDFT_LADDER_OPERANDS = tf32 | bf16: the low rungs of the precision
+    // ladder round the operands of the 1D operator products as a tensor-core
+    // MMA of that input format would (matrix-free kernel, orders 2, 4, 5)
+    const char *lo = std::getenv("INVDFT_LADDER_OPERANDS");
+    const std::string lov = lo ? lo : "fp32";
+    check(lov == "fp32" || lov == "tf32" || lov == "bf16", "INVDFT_LADDER_OPERANDS must be fp32, tf32 or bf16");
+    ladder_operands = lov == "tf32" ? 1 : (lov == "bf16" ? 2 : 0);
+    check(ladder_operands == 0 || (hx_variant == 3 && (n1 == 3 || n1 == 5 || n1 == 6)),
+          "INVDFT_LADDER_OPERANDS=tf32|bf16 needs the matrix-free kernel and FE order 2, 4 or 5");
     for (int &v : sf_tuned) v = -1;
   }
   fe.inv_sqrt_mass = invsqrtM.p; fe.sqrt_mass = sqrtM.p;
@@ -554,9 +617,9 @@ void Context::alloc_state() {
   Yb.alloc((size_t)nn * N);
   Zb.alloc((size_t)nn * N);
   Wb.alloc((size_t)nn * N);
-  Ycell.alloc((size_t)nc * nd * std::max(maxB, 2) + 2);   // +2: 16-byte rounded segment copies
+  Ycell.alloc((size_t)n_slots * std::max(maxB, 2) + 2);   // +2: 16-byte rounded segment copies
   vks.alloc(nc * nq);
-  if (hx_variant == 3) vj.alloc(nc * nq);
+  if (hx_variant == 3) vj.alloc(2 * nc * nq);   // [nc][nq], then [nq][nc]
   rho.alloc(nc * nq);
   u.alloc(nc * nq);
   psi.alloc((size_t)nn * N);
@@ -611,14 +674,16 @@ int Context::sf_shape(const double *d_x, int Bw) {
   INVDFT_CUDA(cudaEventCreate(&b));
   float best = 0.f;
   int arg = cand.back();
+  const int reps = Bw <= 4 ? 6 : 2;   // short launches: more of them against timer noise
   for (size_t k = 0; k < cand.size(); ++k) {
     launch_hx_cell_sf(fe, sfm, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, cand[k], stream);
     INVDFT_CUDA(cudaEventRecord(a, stream));
-    for (int r = 0; r < 2; ++r) launch_hx_cell_sf(fe, sfm, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, cand[k], stream);
+    for (int r = 0; r < reps; ++r) launch_hx_cell_sf(fe, sfm, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, cand[k], stream);
     INVDFT_CUDA(cudaEventRecord(b, stream));
     INVDFT_CUDA(cudaEventSynchronize(b));
     float ms = 0.f;
     INVDFT_CUDA(cudaEventElapsedTime(&ms, a, b));
+    if (trace) std::fprintf(stderr, "sf autotune: width %d shape %d %.4f ms\n", Bw, cand[k], ms / reps);
     if (k == 0 || ms < best) {
       best = ms;
       arg = cand[k];
@@ -633,7 +698,11 @@ void Context::cell_gemm(const double *d_x, int Bw, bool low) {
   const int shape = (!low && hx_variant == 3) ? sf_shape(d_x, Bw) : 0;   // tuning stays outside the timing
   const bool rec = profile && ev_used + 2 <= (int)ev_pool.size();
   if (rec) INVDFT_CUDA(cudaEventRecord(ev_pool[ev_used], stream));
-  if (low && hx_variant == 3) launch_hx_cell_sf_f32(fe, sfm32, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
+  if (low && hx_variant == 3 && in_filter && ladder_operands == 1)
+    launch_hx_cell_sf_tc(fe, sfm_tf32, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
+  else if (low && hx_variant == 3 && in_filter && ladder_operands == 2)
+    launch_hx_cell_sf_tc(fe, sfm_bf16, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
+  else if (low && hx_variant == 3) launch_hx_cell_sf_f32(fe, sfm32, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
   else if (low) launch_hx_cell_dmma_f32(fe, H32.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
   else if (hx_variant == 3) launch_hx_cell_sf(fe, sfm, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, shape, stream);
   else if (hx_variant == 0) launch_hx_cell_dmma(fe, H.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
@@ -683,7 +752,7 @@ void Context::profile_end(invdft_force_stats *st) {
 
 void Context::hx(const double *d_x, double *d_y, int Bw) {
   if (!have_H) throw StatusError(INVDFT_NOT_READY, "no potential set");
-  Ycell.ensure((size_t)nc * nd * Bw + 2);
+  Ycell.ensure((size_t)n_slots * Bw + 2);
   cell_gemm(d_x, Bw);
   AsmEpilogue epi;
   epi.kind = AsmEpilogue::STORE;
@@ -744,7 +813,10 @@ bool Context::needs_cell_matrices() const {
 void Context::set_potential_device(double *d_pot) {
   launch_distribute(cchild.rows.p, cchild.ptr.p, cchild.masters.p, cchild.w.p, cchild.n, d_pot, 1, stream);
   launch_child_to_parent_quad(cv, d_pot, v_base.p, v_lda.p, prm.factor_lda, vks.p, nc * nq, stream);
-  if (hx_variant == 3) launch_mul(vks.p, jxw.p, vj.p, nc * nq, stream);
+  if (hx_variant == 3) {
+    launch_mul(vks.p, jxw.p, vj.p, nc * nq, stream);
+    launch_transpose(vj.p, vj.p + nc * nq, nc, nq, stream);
+  }
   if (needs_cell_matrices()) {
     H.ensure((size_t)nc * ((nd + 1) / 2) * 2 * ldh);
     launch_build_cell_h(fe, vks.p, jxw.p, Kref.p, H.p, stream);
@@ -947,7 +1019,9 @@ void Context::solve_eigen(double *d_pot, invdft_force_stats *st) {
       a0 = eig.front();
       a = eig.back();
     }
+    in_filter = true;   // operand rounding (ladder_operands) applies to the filter's products only
     chfsi_pass(a, b, a0, res, low);
+    in_filter = false;
     mu = fermi_energy(eig, n_electrons, kT);
     occ.resize(N);
     int homo = 0;
@@ -1325,16 +1399,30 @@ void Context::minres_core(const double *d_rhs, double *d_x, double tol, int maxi
   INVDFT_CUDA(cudaMemsetAsync(m_w.p, 0, v * sizeof(double), stream));
   INVDFT_CUDA(cudaMemsetAsync(m_w2.p, 0, v * sizeof(double), stream));
   std::vector<int> act(64);
+  std::vector<int> width_iters(65, 0);   // iterations run at each block width (trace)
+  std::vector<double> width_ms(65, 0.0); // device time of the segments at each width (trace)
+  cudaEvent_t seg_ev[2] = {nullptr, nullptr};
+  int seg_width = 0;
+  if (trace) {
+    INVDFT_CUDA(cudaEventCreate(&seg_ev[0]));
+    INVDFT_CUDA(cudaEventCreate(&seg_ev[1]));
+  }
   const int check_every = 8;
   bool need_v = true;
-  if (!m_ticket.p) {
-    m_ticket.alloc(1);
+  if (!m_ticket.p) {   // [0]: the fused update1's, [1]: the assembly's alpha reduction
+    m_ticket.alloc(2);
     m_ticket.zero(stream);
   }
   for (int itn = 1; itn <= maxit; ++itn) {
     if ((itn - 1) % check_every == 0) {
+      if (trace) INVDFT_CUDA(cudaEventRecord(seg_ev[1], stream));
       INVDFT_CUDA(cudaMemcpyAsync(act.data(), st.active, sizeof(int) * Bc, cudaMemcpyDeviceToHost, stream));
       INVDFT_CUDA(cudaStreamSynchronize(stream));
+      if (trace) {   // the segment since the last check ran at width seg_width
+        float ms = 0.0f;
+        if (seg_width > 0) INVDFT_CUDA(cudaEventElapsedTime(&ms, seg_ev[0], seg_ev[1]));
+        width_ms[seg_width] += ms;
+      }
       std::vector<int> keep;
       for (int k = 0; k < Bc; ++k)
         if (act[k]) keep.push_back(k);
@@ -1343,6 +1431,10 @@ void Context::minres_core(const double *d_rhs, double *d_x, double tol, int maxi
         compact(keep);
         need_v = true;   // v is not part of the re-packed state
       }
+    }
+    if (trace && (itn - 1) % check_every == 0) {
+      seg_width = Bc;
+      INVDFT_CUDA(cudaEventRecord(seg_ev[0], stream));
     }
     if (need_v) launch_minres_v(m_y.p, st, m_v.p, nn, Bc, stream);   // else left by the fused update2
     need_v = false;
@@ -1354,10 +1446,15 @@ void Context::minres_core(const double *d_rhs, double *d_x, double tol, int maxi
     epi.eps = eps_c.p;
     epi.minres_coef = st.coef1;
     epi.dot_partial = partial.p;
+    if (minres_fused) {   // alpha reduced by the assembly's last CTA
+      epi.dot_out = st.alfa;
+      epi.dot_ticket = m_ticket.p + 1;
+    }
     const int nparts = launch_hx_assemble(fe, Ycell.p, m_yn.p, Bc, epi, nblocks_red, stream);
-    launch_reduce_partials(partial.p, nparts, Bc, st.alfa, stream);
+    if (nparts > 0) launch_reduce_partials(partial.p, nparts, Bc, st.alfa, stream);
     n_hx++;
     n_hx_cols += Bc;
+    width_iters[Bc]++;
     if (minres_fused) {
       launch_minres_update1_fused(m_r1.p, m_r2.p, m_y.p, m_yn.p, diagA.p, st, nn, Bc, partial.p, nblocks_red,
                                   m_ticket.p, stream);
@@ -1375,6 +1472,17 @@ void Context::minres_core(const double *d_rhs, double *d_x, double tol, int maxi
   INVDFT_CUDA(cudaStreamSynchronize(stream));
   for (int k = 0; k < Bc; ++k) iters_full[cmap[k]] = it_now[k];
   iters = iters_full;
+  if (trace) {
+    // iterations and device ms per iteration at each width (the segments end at
+    // the host checks; the last, partial segment is not timed)
+    std::fprintf(stderr, "minres%s: iterations per block width:", low ? " (FP32 operator)" : "");
+    for (int w = 1; w <= 64; ++w)
+      if (width_iters[w])
+        std::fprintf(stderr, " %d:%d(%.3f ms/it)", w, width_iters[w], width_ms[w] / std::max(width_iters[w], 1));
+    std::fprintf(stderr, "\n");
+    cudaEventDestroy(seg_ev[0]);
+    cudaEventDestroy(seg_ev[1]);
+  }
 }
 
 // One launch of each kernel of the evaluation on full-size buffers, for
@@ -1409,8 +1517,19 @@ void Context::kernel_probe() {
   INVDFT_CUDA(cudaMemcpyAsync(m_scal.p, ones.data(), sizeof(double) * ones.size(), cudaMemcpyHostToDevice, stream));
   INVDFT_CUDA(cudaMemcpyAsync(m_flags.p, flags.data(), sizeof(int) * flags.size(), cudaMemcpyHostToDevice, stream));
   m_xc.ensure((size_t)nn * N);
-  launch_minres_update1(m_r1.p, m_r2.p, m_y.p, m_b.p, diagA.p, st, nn, N, partial.p, nblocks_red, stream);
-  launch_minres_update2(m_xc.p, m_w.p, m_w2.p, m_b.p, st, nn, N, stream);
+  if (minres_fused) {   // the launches an iteration makes by default
+    if (!m_ticket.p) {
+      m_ticket.alloc(2);
+      m_ticket.zero(stream);
+    }
+    m_v.ensure((size_t)nn * N);
+    launch_minres_update1_fused(m_r1.p, m_r2.p, m_y.p, m_b.p, diagA.p, st, nn, N, partial.p, nblocks_red,
+                                m_ticket.p, stream);
+    launch_minres_update2v(m_xc.p, m_w.p, m_w2.p, m_v.p, m_y.p, st, nn, N, stream);
+  } else {
+    launch_minres_update1(m_r1.p, m_r2.p, m_y.p, m_b.p, diagA.p, st, nn, N, partial.p, nblocks_red, stream);
+    launch_minres_update2(m_xc.p, m_w.p, m_w2.p, m_b.p, st, nn, N, stream);
+  }
   INVDFT_CUDA(cudaStreamSynchronize(stream));
   invalidate_forward();
   psi_ready = false;

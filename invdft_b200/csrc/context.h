@@ -44,10 +44,11 @@ class Context {
   // parent data
   DevBuf<double> phi, Kref, cell_h, jxw, v_base, v_lda, rho_t, weight;
   DevBuf<int> cell_nodes, cell_map;
+  DevBuf<int> cell_map_sf;               // the matrix-free kernel's gather map (compact constrained rows)
+  DevBuf<int> cell_map_t, d_slot_of_t;   // [nd][nc] copies (narrow blocks of the matrix-free kernel)
   Cons cpsi, cadj, cchild;
   DevBuf<double> cons_gw;
   DevBuf<int> d_slot_of, d_dptr, d_err, d_zptr;
-  DevBuf<double> d_z;
   int nhang = 0;
   int ldh = 0;
   // cell products: 3 matrix-free sum factorisation (default), 0 FP64 tensor core
@@ -60,16 +61,21 @@ class Context {
   int sf_shape(const double *d_x, int Bw);
   SfMats sfm{};                    // reference-element matrices of the matrix-free variant
   SfMatsT<float> sfm32{};          // the same in FP32 (low rungs of the precision ladder)
+  SfMatsT<Tf32Operand> sfm_tf32{}; // ... with TF32- / BF16-rounded products (ladder_operands 1 / 2)
+  SfMatsT<Bf16Operand> sfm_bf16{};
+  int ladder_operands = 0;         // filter products of the low rungs: 0 FP32, 1 TF32 operands, 2 BF16 operands
+  bool in_filter = false;          // a Chebyshev filter pass is running
   DevBuf<double> vj;               // [nc][nq] v_KS * JxW (matrix-free variant)
-  DevBuf<int> d_midx;              // compact numbering of the masters of hanging nodes
-  DevBuf<double> d_mz;             // [nmast][64] per-master hanging contributions
+  DevBuf<int> d_mslot;             // [nmast] the slot of each master that holds its hanging contributions
+  int64_t n_slots = 0;             // result slots of a cell product (per column)
   int n_masters = 0;
   // constraint groups (rows with identical master lists) and master pair lists
   DevBuf<int> d_g_rptr, d_g_rows, d_g_hrow, d_g_m0, d_g_nm, d_g_poff, d_mp_ptr, d_mp_idx;
   DevBuf<double> d_gpart;          // [npairs][64] per-(group, master) partial sums
   DevBuf<int64_t> d_g_woff;        // per-group start of its weight block
-  DevBuf<double> d_g_gw, d_g_w;    // group weights, Lowdin-scaled and plain
-  DevBuf<double> d_hvg;            // [ncons][64] pre-gathered constrained rows (matrix-free variant)
+  DevBuf<double> d_g_w, d_g_wt;    // distinct group weight blocks, [row][master] and [master][row]
+  int n_weight_blocks = 0;
+  DevBuf<double> d_hvg;            // [nhang+1][64] pre-gathered hanging rows and a zero row (matrix-free variant)
   bool needs_cell_matrices() const;
   void check_device_error();
   DevBuf<double> sqrtM, invsqrtM, diagA, diagSqrtA;

@@ -6,6 +6,8 @@
 // column j of H_e with unit stride.
 #include "kernels.cuh"
 
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <cstdlib>
 #include <string>
@@ -341,6 +343,25 @@ __device__ __forceinline__ int sf_point(int L, int k) {
 
 __device__ __forceinline__ double sf_fma(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float sf_fma(float a, float b, float c) { return fmaf(a, b, c); }
+// Products that feed an addition are written as __dmul_rn / __fmul_rn so the
+// compiler cannot contract them into an FMA with that addition: every launch
+// shape of the cell kernel then rounds identically, whatever its code layout.
+__device__ __forceinline__ double sf_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float sf_mul(float a, float b) { return __fmul_rn(a, b); }
+template <int M> __device__ __forceinline__ TcOperand<M> sf_mul(TcOperand<M> a, TcOperand<M> b) {
+  return __fmul_rn(a.v, b.v);
+}
+__device__ __forceinline__ float tf32_round(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+__device__ __forceinline__ Tf32Operand sf_fma(Tf32Operand a, Tf32Operand b, Tf32Operand c) {
+  return fmaf(tf32_round(a.v), tf32_round(b.v), c.v);
+}
+__device__ __forceinline__ Bf16Operand sf_fma(Bf16Operand a, Bf16Operand b, Bf16Operand c) {
+  return fmaf(__bfloat162float(__float2bfloat16_rn(a.v)), __bfloat162float(__float2bfloat16_rn(b.v)), c.v);
+}
 
 template <int N, int DIR, typename T>
 __device__ __forceinline__ void sf_load(const T *a, int L, int p, T (&r)[N]) {
@@ -463,10 +484,15 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
   const int64_t e = (int64_t)blockIdx.x * G + g;
   const int b = blockIdx.y * C + c;
   const bool act = e < fe.nc && b < B;
+  // index of (cell e, local l) in the per-cell arrays: [nd][nc] (transposed
+  // copies, contiguous over the CTA's cells) when the CTA holds several cells
+  const bool trn = G > 1;
+  auto at = [&](int l) -> int64_t { return trn ? (int64_t)l * fe.nc + e : e * N3 + l; };
+  const double *vjv = trn ? vj + fe.nc * N3 : vj;
   if (PRE) {
 #pragma unroll
     for (int k = 0; k < N; ++k)
-      cp_async8(&Vs[sf_point<N, 2>(L, k) * 16 + p], act ? &vj[e * N3 + L + N2 * k] : vj, act);
+      cp_async8(&Vs[sf_point<N, 2>(L, k) * 16 + p], act ? &vjv[at(L + N2 * k)] : vj, act);
     cp_async_commit();
   }
   const T hh = act ? T(0.5 * fe.cell_h[e]) : T(0);
@@ -476,7 +502,7 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
     if (L % N == k) wa = mt.w[k];
     if (L / N == k) wb = mt.w[k];
   }
-  const T f = hh * wa * wb;
+  const T f = sf_mul(sf_mul(hh, wa), wb);
   T r[N], s[N], gx[N];
   // gather of the z-line L straight into registers: all N node indices, then
   // all 2N independent value loads, then the (rare) hanging rows; phi along z
@@ -485,17 +511,17 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
 #pragma unroll
     for (int k = 0; k < N; ++k) {
       const int l = L + N2 * k;
-      m[k] = act ? (mode == GATHER_PLAIN ? fe.cell_nodes[e * N3 + l] : fe.cell_map[e * N3 + l]) : 0;
+      m[k] = act ? (mode == GATHER_PLAIN ? fe.cell_nodes[e * N3 + l] : (trn ? fe.cell_map_t : fe.cell_map_sf)[at(l)]) : 0;
     }
 #pragma unroll
     for (int k = 0; k < N; ++k) {
       const bool direct = act && m[k] >= 0;
       const double xv = direct ? x[(int64_t)m[k] * B + b] : 0.0;
       const double sc = (direct && mode != GATHER_PLAIN) ? fe.inv_sqrt_mass[m[k]] : 1.0;
-      r[k] = T(xv * sc);
+      r[k] = T(__dmul_rn(xv, sc));
     }
 #pragma unroll
-    for (int k = 0; k < N; ++k)   // constrained rows: pre-gathered by hanging_gather_kernel
+    for (int k = 0; k < N; ++k)   // constrained rows: pre-gathered by group_gather_kernel
       if (act && m[k] < 0) r[k] = T(fe.hvg[(int64_t)(-m[k] - 1) * B + b]);
   }
   sf_phi<N>(mt, r, s);
@@ -510,13 +536,13 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
   sf_store<N, 0>(A, L, p, s);
   sf_dq<N>(mt, s, gx);
 #pragma unroll
-  for (int q = 0; q < N; ++q) gx[q] *= f * mt.w[q];
+  for (int q = 0; q < N; ++q) gx[q] = sf_mul(gx[q], sf_mul(f, mt.w[q]));
   if (GXS) sf_store<N, 0>(Gs, L, p, gx);
   __syncthreads();
   sf_load<N, 1>(A, L, p, r);             // d/dy, weighted, kept for the y back pass
   sf_dq<N>(mt, r, s);
 #pragma unroll
-  for (int q = 0; q < N; ++q) s[q] *= f * mt.w[q];
+  for (int q = 0; q < N; ++q) s[q] = sf_mul(s[q], sf_mul(f, mt.w[q]));
   sf_store<N, 1>(Cs, L, p, s);
   {
     T v[N];
@@ -527,18 +553,19 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
       // the slot indices of the output, into the low half of each used entry
 #pragma unroll
       for (int k = 0; k < N; ++k)
-        cp_async4(&Vs[sf_point<N, 2>(L, k) * 16 + p], act ? &fe.slot_of[e * N3 + L + N2 * k] : fe.slot_of, act);
+        cp_async4(&Vs[sf_point<N, 2>(L, k) * 16 + p], act ? &(trn ? fe.slot_of_t : fe.slot_of)[at(L + N2 * k)] : fe.slot_of,
+                  act);
       cp_async_commit();
     } else {
 #pragma unroll
-      for (int k = 0; k < N; ++k) v[k] = act ? T(vj[e * N3 + L + N2 * k]) : T(0);
+      for (int k = 0; k < N; ++k) v[k] = act ? T(vjv[at(L + N2 * k)]) : T(0);
     }
     sf_load<N, 2>(A, L, p, r);           // d/dz, the z back pass and the potential term
     sf_dq<N>(mt, r, s);
 #pragma unroll
     for (int q = 0; q < N; ++q) {
-      s[q] *= f * mt.w[q];
-      r[q] *= v[q];
+      s[q] = sf_mul(s[q], sf_mul(f, mt.w[q]));
+      r[q] = sf_mul(r[q], v[q]);
     }
     sf_dqt_add<N>(mt, s, r);
     sf_store<N, 2>(Bs, L, p, r);
@@ -566,7 +593,7 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
 #pragma unroll
     for (int k = 0; k < N; ++k) {
       const int sl = PRE ? *reinterpret_cast<const int *>(&Vs[sf_point<N, 2>(L, k) * 16 + p])
-                         : fe.slot_of[e * N3 + L + N2 * k];
+                         : (trn ? fe.slot_of_t : fe.slot_of)[at(L + N2 * k)];
       if (sl >= 0) Ycell[(int64_t)sl * B + b] = double(s[k]);
     }
   }
@@ -734,16 +761,38 @@ __global__ void __launch_bounds__(NT, 1) hx_gemm_bulk_kernel(FeView fe, const do
   }
 }
 
-// One tile of the assembly: node rows r0 .. r0+rows-1 with their direct slots
-// read from segp[sl*B + j - a0] (a shared-memory copy of the tile's slot
-// segment, or the cell results themselves with a0 = 0), their slot ranges
-// from dp,
-// compact master indices from mi (-1: no hanging contributions, else the row
-// of mz), M^-1/2 from ism and the epilogue inputs from t_in/t_prev (all
-// tile-local, row stride B for blocks).  Thread (rr, j) handles column j of
-// rows rr, rr+RR, ... in a fixed order.
+// The last CTA of a grid-wide reduction: out[c] = sum over g < nparts of
+// partial[g*B + c] for c < B (B <= NT).  Every thread of the CTA takes part:
+// thread (group k, column c) sums the partials k, k + R, ... (R = NT / B), then
+// the R group sums of each column are added by a halving tree.  The order is
+// fixed by B and nparts alone, so the result is deterministic.
+__device__ void cta_column_sums(const double *partial, int nparts, int B, double *out, double *red) {
+  const int R = NT / B;
+  const int c = threadIdx.x % B, k = threadIdx.x / B;
+  double v = 0.0;
+  if (k < R)
+    for (int g = k; g < nparts; g += R) v += __ldcg(&partial[(int64_t)g * B + c]);
+  red[threadIdx.x] = v;
+  __syncthreads();
+  int span = 1;
+  while (span < R) span <<= 1;
+  for (int h = span >> 1; h > 0; h >>= 1) {
+    if (k < h && k + h < R) red[k * B + c] += red[(k + h) * B + c];
+    __syncthreads();
+  }
+  if (threadIdx.x < B) out[threadIdx.x] = red[threadIdx.x];
+  __syncthreads();
+}
+
+// One tile of the assembly: node rows r0 .. r0+rows-1 with their slots read
+// from segp[sl*B + j - a0] (a shared-memory copy of the tile's slot segment, or
+// the cell results themselves with a0 = 0) -- a master of hanging nodes has its
+// summed hanging contributions in its last slot -- their slot ranges from dp,
+// M^-1/2 from ism and the epilogue inputs from t_in/t_prev (all tile-local, row
+// stride B for blocks).  Thread (rr, j) handles column j of rows rr, rr+RR, ...
+// in a fixed order.
 __device__ __forceinline__ void assemble_tile_rows(const FeView &fe, const double *segp, int64_t a0,
-                                                   const int *dp, const int *mi, const double *ism,
+                                                   const int *dp, const double *ism,
                                                    const double *t_in, const double *t_prev, int64_t r0, int rows,
                                                    double *__restrict__ out, int B, const AsmEpilogue &epi,
                                                    double &dot) {
@@ -753,10 +802,8 @@ __device__ __forceinline__ void assemble_tile_rows(const FeView &fe, const doubl
   for (int lr = rr; lr < rows; lr += RR) {
     const int64_t n = r0 + lr;
     const int d0 = dp[lr], d1 = dp[lr + 1];
-    double acc = 0.0;
+    double acc = 0.0;   // a master's hanging contributions are its last slot
     for (int sl = d0; sl < d1; ++sl) acc += segp[(int64_t)sl * B + j - a0];
-    const int m = mi[lr];
-    if (m >= 0) acc += fe.mz[(int64_t)m * B + j];
     acc *= ism[lr];
     const int64_t idx = n * B + j;
     const int li = lr * B + j;
@@ -795,28 +842,28 @@ constexpr int kAsmBlk = 4;   // ... of an epilogue block (TR B <= 4 NT)
 constexpr int kAsmSeg = 8;   // ... of a staged slot segment (cap B = 2 TR B <= 8 NT)
 
 // ---------------------------------------------------------------------------
-// HX, part 2 (tiled): a CTA owns TR consecutive nodes, whose direct slots form
-// one contiguous segment [dptr[r0], dptr[r0+TR]).  The segment is streamed
-// into shared memory with coalesced loads and the per-node sums are taken from
-// there; a master of hanging nodes adds its pre-summed contribution
-// mz[midx[n]] (one load).  Thread (rr, j) handles column j of nodes r0+rr,
+// HX, part 2 (tiled): a CTA owns TR consecutive nodes, whose slots form one
+// contiguous segment [dptr[r0], dptr[r0+TR]).  The segment is streamed into
+// shared memory with coalesced loads and the per-node sums are taken from
+// there; a master of hanging nodes finds its pre-summed contribution in its
+// last slot, written by the master-sum pass.  Thread (rr, j) handles column j of nodes r0+rr,
 // r0+rr+RR, ... (fixed order), so the MINRES dot partials are deterministic.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(NT, 4) hx_assemble_tile_kernel(FeView fe, const double *__restrict__ Ycell,
                                                               double *__restrict__ out, int B, AsmEpilogue epi,
                                                               int TR, int cap_slots) {
-  // shared layout: seg [cap][B] | s_in [TR][B] | s_prev [TR][B] | ism [TR] | dp [TR+1] | mi [TR]
+  // shared layout: seg [cap][B] | s_in [TR][B] | s_prev [TR][B] | ism [TR] | dp [TR+1]
   extern __shared__ double sm_asm[];
   double *seg = sm_asm;
   double *s_in = seg + (size_t)cap_slots * B;
   double *s_prev = s_in + (size_t)TR * B;
   double *ism = s_prev + (size_t)TR * B;
   int *dp = reinterpret_cast<int *>(ism + TR);
-  int *mi = dp + TR + 1;
   __shared__ double red[NT];
+  __shared__ bool last;
   const int64_t r0 = (int64_t)blockIdx.x * TR;
-  if (r0 >= fe.nnodes) return;   // grid sized by the caller: never past the last node
-  const int rows = (int)min((int64_t)TR, fe.nnodes - r0);
+  // the grid is sized by the caller (ceil(nnodes / TR)), so rows >= 1
+  const int rows = (int)max((int64_t)0, min((int64_t)TR, fe.nnodes - r0));
   const bool need_in = epi.kind == AsmEpilogue::CHEB || epi.kind == AsmEpilogue::VMULT ||
                        epi.kind == AsmEpilogue::MINRES;
   const bool need_prev = (epi.kind == AsmEpilogue::CHEB && epi.prev) || epi.kind == AsmEpilogue::MINRES;
@@ -826,13 +873,12 @@ __global__ void __launch_bounds__(NT, 4) hx_assemble_tile_kernel(FeView fe, cons
   const int s0 = fe.dptr[r0], s1 = fe.dptr[r0 + rows];
   const bool staged = (s1 - s0) <= cap_slots;
   const int tid = threadIdx.x, nb = rows * B, ns = (s1 - s0) * B;
-  int v_dp[kAsmRow], v_mi[kAsmRow];
+  int v_dp[kAsmRow];
   double v_ism[kAsmRow], v_in[kAsmBlk], v_pr[kAsmBlk], v_sg[kAsmSeg];
 #pragma unroll
   for (int u = 0; u < kAsmRow; ++u) {
     const int i = tid + u * NT;
     v_dp[u] = i <= rows ? fe.dptr[r0 + i] : 0;
-    v_mi[u] = i < rows ? fe.midx[r0 + i] : -1;
     v_ism[u] = i < rows ? fe.inv_sqrt_mass[r0 + i] : 0.0;
   }
 #pragma unroll
@@ -850,10 +896,7 @@ __global__ void __launch_bounds__(NT, 4) hx_assemble_tile_kernel(FeView fe, cons
   for (int u = 0; u < kAsmRow; ++u) {
     const int i = tid + u * NT;
     if (i <= rows) dp[i] = v_dp[u];
-    if (i < rows) {
-      mi[i] = v_mi[u];
-      ism[i] = v_ism[u];
-    }
+    if (i < rows) ism[i] = v_ism[u];
   }
 #pragma unroll
   for (int u = 0; u < kAsmBlk; ++u) {
@@ -870,7 +913,7 @@ __global__ void __launch_bounds__(NT, 4) hx_assemble_tile_kernel(FeView fe, cons
   }
   __syncthreads();
   double dot = 0.0;
-  assemble_tile_rows(fe, staged ? seg : Ycell, staged ? (int64_t)s0 * B : 0, dp, mi, ism, s_in, s_prev, r0, rows,
+  assemble_tile_rows(fe, staged ? seg : Ycell, staged ? (int64_t)s0 * B : 0, dp, ism, s_in, s_prev, r0, rows,
                      out, B, epi, dot);
   if (epi.kind == AsmEpilogue::MINRES) {
     const int RR = NT / B;
@@ -880,6 +923,18 @@ __global__ void __launch_bounds__(NT, 4) hx_assemble_tile_kernel(FeView fe, cons
       double sum = 0.0;
       for (int q = 0; q < RR; ++q) sum += red[q * B + threadIdx.x];
       epi.dot_partial[(int64_t)blockIdx.x * B + threadIdx.x] = sum;
+    }
+    if (epi.dot_ticket) {
+      // the last CTA to finish (ticket taken after a fence) reduces the
+      // partials, each column by one warp in a fixed order
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) last = atomicAdd(epi.dot_ticket, 1u) == gridDim.x - 1;
+      __syncthreads();
+      if (!last) return;
+      __threadfence();
+      cta_column_sums(epi.dot_partial, (int)gridDim.x, B, epi.dot_out, red);
+      if (threadIdx.x == 0) *epi.dot_ticket = 0u;
     }
   }
 }
@@ -899,12 +954,12 @@ __global__ void __launch_bounds__(NT, 4) hx_assemble_tile_kernel(FeView fe, cons
 // ---------------------------------------------------------------------------
 struct AsmStage {
   double *seg, *in, *prev, *ism;
-  int *dp, *mi;
+  int *dp;
 };
 
 __device__ __forceinline__ AsmStage asm_stage(unsigned char *base, int st, int TR, int cap, int B) {
   const size_t seg_n = (size_t)cap * B + 2, blk = (size_t)TR * B;
-  const size_t stage_bytes = 8 * (seg_n + 2 * blk + TR) + 4 * 2 * ((size_t)TR + 4);
+  const size_t stage_bytes = 8 * (seg_n + 2 * blk + TR) + 4 * ((size_t)TR + 4);
   double *p = reinterpret_cast<double *>(base + (size_t)st * ((stage_bytes + 127) & ~(size_t)127));
   AsmStage s;
   s.seg = p;
@@ -912,7 +967,6 @@ __device__ __forceinline__ AsmStage asm_stage(unsigned char *base, int st, int T
   s.prev = s.in + blk;
   s.ism = s.prev + blk;
   s.dp = reinterpret_cast<int *>(s.ism + TR);
-  s.mi = s.dp + TR + 4;
   return s;
 }
 
@@ -939,7 +993,7 @@ __global__ void __launch_bounds__(NT) hx_assemble_bulk_kernel(FeView fe, const d
     const int64_t r0 = (blockIdx.x + i * G) * TR;
     AsmStage S = asm_stage(sm_ab, (int)(i & 1), TR, cap, B);
     uint64_t *bar = &bars[i & 1];
-    uint32_t bytes = 2u * 4u * (uint32_t)(TR + 4) + 8u * (uint32_t)TR;
+    uint32_t bytes = 4u * (uint32_t)(TR + 4) + 8u * (uint32_t)TR;
     if (need_in) bytes += 8u * (uint32_t)TR * B;
     if (need_prev) bytes += 8u * (uint32_t)TR * B;
     const bool staged = s1 - s0 <= cap;
@@ -947,7 +1001,6 @@ __global__ void __launch_bounds__(NT) hx_assemble_bulk_kernel(FeView fe, const d
     if (staged) bytes += 8u * (uint32_t)(a1 - a0);
     mbar_expect_tx(bar, bytes);
     bulk_g2s(S.dp, fe.dptr + r0, 4u * (TR + 4), bar);
-    bulk_g2s(S.mi, fe.midx + r0, 4u * (TR + 4), bar);
     bulk_g2s(S.ism, fe.inv_sqrt_mass + r0, 8u * TR, bar);
     if (need_in) bulk_g2s(S.in, epi.in + r0 * B, 8u * TR * B, bar);
     if (need_prev) bulk_g2s(S.prev, epi.prev + r0 * B, 8u * TR * B, bar);
@@ -990,7 +1043,7 @@ __global__ void __launch_bounds__(NT) hx_assemble_bulk_kernel(FeView fe, const d
     const int s0 = S.dp[0], s1 = S.dp[TR];
     const bool staged = s1 - s0 <= cap;
     const int64_t a0 = staged ? (((int64_t)s0 * B) & ~(int64_t)1) : 0;
-    assemble_tile_rows(fe, staged ? S.seg : Ycell, a0, S.dp, S.mi, S.ism, S.in, S.prev, r0, TR, out, B, epi, dot);
+    assemble_tile_rows(fe, staged ? S.seg : Ycell, a0, S.dp, S.ism, S.in, S.prev, r0, TR, out, B, epi, dot);
     __syncthreads();
     if (threadIdx.x == 0 && i + 2 < cnt) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1001,7 +1054,7 @@ __global__ void __launch_bounds__(NT) hx_assemble_bulk_kernel(FeView fe, const d
   const int64_t rt = nfull * TR;
   if (rt < fe.nnodes && blockIdx.x == nfull % G) {
     const int rows = (int)(fe.nnodes - rt);
-    assemble_tile_rows(fe, Ycell, 0, fe.dptr + rt, fe.midx + rt, fe.inv_sqrt_mass + rt,
+    assemble_tile_rows(fe, Ycell, 0, fe.dptr + rt, fe.inv_sqrt_mass + rt,
                        need_in ? epi.in + rt * B : nullptr, need_prev ? epi.prev + rt * B : nullptr, rt, rows,
                        out, B, epi, dot);
   }
@@ -1017,59 +1070,57 @@ __global__ void __launch_bounds__(NT) hx_assemble_bulk_kernel(FeView fe, const d
   }
 }
 
-// z[h][j] = sum of the cell rows of hanging node h (contiguous slots)
-__global__ void hanging_sum_kernel(FeView fe, const double *__restrict__ Ycell, int B) {
-  const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (idx >= (int64_t)fe.nhang * B) return;
-  const int h = (int)(idx / B), j = (int)(idx % B);
+// z[h][j] = sum of the cell rows of hanging node h (its contiguous slots), in slot order
+__device__ __forceinline__ double hanging_row_sum(const FeView &fe, const double *__restrict__ Ycell, int h, int j,
+                                                  int B) {
   double acc = 0.0;
   for (int sl = fe.zptr[h]; sl < fe.zptr[h + 1]; ++sl) acc += Ycell[(int64_t)sl * B + j];
-  fe.z[idx] = acc;
+  return acc;
 }
 
 // What C^T adds to the masters of hanging nodes, in two passes.  One CTA per
-// hanging constraint group reads the group's z rows and weights once into
-// shared memory
-// and writes gpart[g_poff[g] + t][j] = sum_q w[row q, t] z[row q][j] for each
-// of its masters t; then mz[i][j] sums master i's (group, master) partials,
-// both in a fixed order.
-__global__ void __launch_bounds__(NT) group_partial_kernel(FeView fe, int B, int cap) {
-  extern __shared__ double sp[];   // zr [nr][B] | wm [nr][nm]
+// hanging constraint group sums the cell rows of the group's hanging nodes (z,
+// each hanging node belongs to one group) into shared memory, stages the
+// group's weights, and writes gpart[g_poff[g] + t][j] = sum_q w[row q, t] z[row q][j]
+// for each of its masters t; then master_sum_kernel sums master i's (group,
+// master) partials into the master's last slot.  Both in a fixed order.
+__global__ void __launch_bounds__(NT) group_partial_kernel(FeView fe, const double *__restrict__ Ycell, int B,
+                                                           int cap) {
+  extern __shared__ double sp[];   // zr [nr][B]
   const int g = blockIdx.x;
   const int nm = fe.g_nm[g], rp0 = fe.g_rptr[g], nr = fe.g_rptr[g + 1] - rp0;
   const int64_t po = fe.g_poff[g];
   const double *w = fe.g_w + fe.g_woff[g];
-  if ((int64_t)nr * (B + nm) > cap) {   // too large to stage: read from global memory
+  if ((int64_t)nr * B > cap) {   // too large to stage: z summed per use from the cell results
     for (int i = threadIdx.x; i < nm * B; i += blockDim.x) {
       const int t = i / B, j = i - t * B;
       double acc = 0.0;
-      for (int q = 0; q < nr; ++q) acc = fma(w[q * nm + t], fe.z[(int64_t)fe.g_hrow[rp0 + q] * B + j], acc);
+      for (int q = 0; q < nr; ++q) acc = fma(w[q * nm + t], hanging_row_sum(fe, Ycell, fe.g_hrow[rp0 + q], j, B), acc);
       fe.gpart[(po + t) * B + j] = acc;
     }
     return;
   }
-  double *zr = sp, *wm = sp + (size_t)nr * B;
+  double *zr = sp;
   for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
     const int q = i / B, j = i - q * B;
-    zr[i] = fe.z[(int64_t)fe.g_hrow[rp0 + q] * B + j];
+    zr[i] = hanging_row_sum(fe, Ycell, fe.g_hrow[rp0 + q], j, B);
   }
-  for (int i = threadIdx.x; i < nr * nm; i += blockDim.x) wm[i] = w[i];
   __syncthreads();
   for (int i = threadIdx.x; i < nm * B; i += blockDim.x) {
     const int t = i / B, j = i - t * B;
     double acc = 0.0;
-    for (int q = 0; q < nr; ++q) acc = fma(wm[q * nm + t], zr[q * B + j], acc);
+    for (int q = 0; q < nr; ++q) acc = fma(w[q * nm + t], zr[q * B + j], acc);
     fe.gpart[(po + t) * B + j] = acc;
   }
 }
 
-__global__ void master_sum_kernel(FeView fe, int B) {
+__global__ void master_sum_kernel(FeView fe, int B, double *__restrict__ Ycell) {
   const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (idx >= (int64_t)fe.nmast * B) return;
   const int i = (int)(idx / B), j = (int)(idx - (int64_t)i * B);
   double acc = 0.0;
   for (int q = fe.mp_ptr[i]; q < fe.mp_ptr[i + 1]; ++q) acc += fe.gpart[(int64_t)fe.mp_idx[q] * B + j];
-  fe.mz[idx] = acc;
+  Ycell[(int64_t)fe.mslot[i] * B + j] = acc;
 }
 
 __global__ void scale_rows_kernel(const double *d, const double *x, double *y, int64_t n, int B) {
@@ -1556,14 +1607,7 @@ __global__ void __launch_bounds__(NT) minres_update1_fused_kernel(double *__rest
   __syncthreads();
   if (!last) return;
   __threadfence();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int c = warp; c < B; c += NT / 32) {
-    double v = 0.0;
-    for (int g = lane; g < (int)gridDim.x; g += 32) v += __ldcg(&partial[(int64_t)g * B + c]);
-    v = warp_sum(v);
-    if (lane == 0) st.beta2[c] = v;
-  }
-  __syncthreads();
+  cta_column_sums(partial, (int)gridDim.x, B, st.beta2, red);
   if (threadIdx.x < B) minres_column_scalars(st, threadIdx.x);
   if (threadIdx.x == 0) *ticket = 0u;
 }
@@ -1871,98 +1915,46 @@ void launch_hx_cell_dmma_f32(const FeView &fe, const float *H32, const double *x
   dmma_dispatch<float>(fe, H32, x, Ycell, B, gather_mode, s);
 }
 
-// hvg[r][b] = sum_t gw_t x[master_t][b] for every constrained row r: the
-// Lowdin gather of the hanging (and, as zeros, the Dirichlet) rows, in the
-// FMA order of gather_value, so the matrix-free kernel reads each with one
-// load.  One CTA per constraint group: the group's master rows and weights
-// are read once into shared memory and serve all of its rows.
+// hvg[h][b] = sum_t w_t (M^-1/2 x)[master_t][b] for every hanging row h (compact
+// hanging index), and hvg[nhang][b] = 0 for the Dirichlet entries: the Lowdin
+// gather of the constrained rows, so the matrix-free kernel reads each with one
+// load.  One CTA per hanging constraint group: the group's master values,
+// scaled by M^-1/2, are staged once in shared memory and serve all of its
+// rows; the weights are read from the group's (shared, [master][row]) block.
 __global__ void __launch_bounds__(NT) group_gather_kernel(FeView fe, const double *__restrict__ x, int B,
                                                           int cap) {
-  extern __shared__ double sg[];   // xm [nm][B] | wm [nr][nm]
+  extern __shared__ double sg[];   // xm [nm][B]
   const int g = blockIdx.x;
+  if (g == 0 && threadIdx.x < B) fe.hvg[(int64_t)fe.nhang * B + threadIdx.x] = 0.0;
+  if (g >= fe.ngroup_h) return;   // the launch with no hanging group: the zero row only
   const int nm = fe.g_nm[g], m0 = fe.g_m0[g];
   const int rp0 = fe.g_rptr[g], nr = fe.g_rptr[g + 1] - rp0;
-  const double *gw = fe.g_gw + fe.g_woff[g];
-  if ((int64_t)nm * (B + nr) > cap) {
+  const double *wt = fe.g_wt + fe.g_woff[g];
+  if ((int64_t)nm * B > cap) {
     // a group too large for the shared staging (rows with hundreds of masters
     // after constraint closure): the same sums, read from global memory
     for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
       const int q = i / B, j = i - q * B;
       double v = 0.0;
-      for (int t = 0; t < nm; ++t) v = fma(gw[q * nm + t], x[(int64_t)fe.cons_masters[m0 + t] * B + j], v);
-      fe.hvg[(int64_t)fe.g_rows[rp0 + q] * B + j] = v;
+      for (int t = 0; t < nm; ++t) {
+        const int mt = fe.cons_masters[m0 + t];
+        v = fma(wt[t * nr + q], __dmul_rn(x[(int64_t)mt * B + j], fe.inv_sqrt_mass[mt]), v);
+      }
+      fe.hvg[(int64_t)fe.g_hrow[rp0 + q] * B + j] = v;
     }
     return;
   }
-  double *xm = sg, *wm = sg + (size_t)nm * B;
   for (int i = threadIdx.x; i < nm * B; i += blockDim.x) {
     const int t = i / B, j = i - t * B;
-    xm[i] = x[(int64_t)fe.cons_masters[m0 + t] * B + j];
+    const int mt = fe.cons_masters[m0 + t];
+    sg[i] = __dmul_rn(x[(int64_t)mt * B + j], fe.inv_sqrt_mass[mt]);
   }
-  for (int i = threadIdx.x; i < nr * nm; i += blockDim.x) wm[i] = gw[i];
   __syncthreads();
   for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
     const int q = i / B, j = i - q * B;
     double v = 0.0;
-    for (int t = 0; t < nm; ++t) v = fma(wm[q * nm + t], xm[t * B + j], v);
-    fe.hvg[(int64_t)fe.g_rows[rp0 + q] * B + j] = v;
-  }
-}
-
-// Narrow blocks (B <= 8: the tail of the MINRES iterations, small meshes): one warp per
-// constraint group instead of a CTA, eight groups per CTA, so the launch fits
-// in one wave and a group's few rows do not idle a whole CTA.  The sums run in
-// the same order as the CTA-per-group kernels, so results are bitwise equal.
-constexpr int kWarpGroupMaxB = 8;
-constexpr int kWarpStageM = 64;   // masters staged per warp (larger groups read global memory)
-
-__global__ void __launch_bounds__(NT) group_gather_warp_kernel(FeView fe, const double *__restrict__ x, int B) {
-  __shared__ double xs[NT / 32][kWarpStageM * kWarpGroupMaxB];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = blockIdx.x * (NT / 32) + warp;
-  if (g >= fe.ngroup) return;   // the whole warp leaves; only warp-level syncs below
-  const int nm = fe.g_nm[g], m0 = fe.g_m0[g];
-  const int rp0 = fe.g_rptr[g], nr = fe.g_rptr[g + 1] - rp0;
-  const double *gw = fe.g_gw + fe.g_woff[g];
-  double *xm = xs[warp];
-  const bool staged = nm <= kWarpStageM && nm * B <= fe.g_stage;
-  if (staged)
-    for (int i = lane; i < nm * B; i += 32) {
-      const int t = i / B, j = i - t * B;
-      xm[i] = x[(int64_t)fe.cons_masters[m0 + t] * B + j];
-    }
-  __syncwarp();
-  for (int i = lane; i < nr * B; i += 32) {
-    const int q = i / B, j = i - q * B;
-    double v = 0.0;
-    for (int t = 0; t < nm; ++t)
-      v = fma(gw[q * nm + t], staged ? xm[t * B + j] : x[(int64_t)fe.cons_masters[m0 + t] * B + j], v);
-    fe.hvg[(int64_t)fe.g_rows[rp0 + q] * B + j] = v;
-  }
-}
-
-__global__ void __launch_bounds__(NT) group_partial_warp_kernel(FeView fe, int B) {
-  __shared__ double zs[NT / 32][kGroupRows * kWarpGroupMaxB];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = blockIdx.x * (NT / 32) + warp;
-  if (g >= fe.ngroup_h) return;
-  const int nm = fe.g_nm[g], rp0 = fe.g_rptr[g], nr = fe.g_rptr[g + 1] - rp0;
-  const int64_t po = fe.g_poff[g];
-  const double *w = fe.g_w + fe.g_woff[g];
-  double *zr = zs[warp];
-  const bool staged = nr * B <= fe.g_stage;
-  if (staged)
-    for (int i = lane; i < nr * B; i += 32) {
-      const int q = i / B, j = i - q * B;
-      zr[i] = fe.z[(int64_t)fe.g_hrow[rp0 + q] * B + j];
-    }
-  __syncwarp();
-  for (int i = lane; i < nm * B; i += 32) {
-    const int t = i / B, j = i - t * B;
-    double acc = 0.0;
-    for (int q = 0; q < nr; ++q)
-      acc = fma(w[q * nm + t], staged ? zr[q * B + j] : fe.z[(int64_t)fe.g_hrow[rp0 + q] * B + j], acc);
-    fe.gpart[(po + t) * B + j] = acc;
+    for (int t = 0; t < nm; ++t) v = fma(wt[t * nr + q], sg[t * B + j], v);
+    fe.hvg[(int64_t)fe.g_hrow[rp0 + q] * B + j] = v;
   }
 }
 
@@ -2001,30 +1993,17 @@ static void hx_sf_dispatch(const FeView &fe, const SfMats &mt, const double *vj,
   }
 }
 
-// INVDFT_GROUP_WARP=0 keeps the CTA-per-group constraint kernels at every width
-static bool group_warp_enabled() {
-  static const bool on = [] {
-    const char *v = std::getenv("INVDFT_GROUP_WARP");
-    return !(v && std::string(v) == "0");
-  }();
-  return on;
-}
-
 static void launch_group_gather(const FeView &fe, const double *x, int B, int gather_mode, cudaStream_t s) {
-  if (gather_mode != GATHER_PLAIN && fe.ngroup > 0 && B <= kWarpGroupMaxB && group_warp_enabled()) {
-    group_gather_warp_kernel<<<ceil_div(fe.ngroup, NT / 32), NT, 0, s>>>(fe, x, B);
-    INVDFT_LAUNCH_CHECK();
-    return;
-  }
   if (gather_mode != GATHER_PLAIN && fe.ngroup > 0) {
     // staging capacity: the largest group's need, at most fe.g_stage doubles
-    const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnm, 1) * (B + fe.g_maxnr), fe.g_stage);
+    const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnm, 1) * B, fe.g_stage);
     static bool attr = false;
     if (!attr) {
       INVDFT_CUDA(cudaFuncSetAttribute(group_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
       attr = true;
     }
-    group_gather_kernel<<<fe.ngroup, NT, sizeof(double) * (size_t)cap, s>>>(fe, x, B, cap);
+    // the hanging groups; block 0 also writes the zero row
+    group_gather_kernel<<<std::max(fe.ngroup_h, 1), NT, sizeof(double) * (size_t)cap, s>>>(fe, x, B, cap);
     INVDFT_LAUNCH_CHECK();
   }
 }
@@ -2042,6 +2021,26 @@ void launch_hx_cell_sf_f32(const FeView &fe, const SfMatsT<float> &mt, const dou
     case 8: hx_sf_n<8, 1, false, float>(fe, mt, vj, x, Ycell, B, gather_mode, s); break;
     default: throw StatusError(5, "matrix-free HX supports FE orders 1..7");
   }
+}
+
+template <typename T>
+static void hx_sf_tc(const FeView &fe, const SfMatsT<T> &mt, const double *vj, const double *x, double *Ycell,
+                     int B, int gather_mode, cudaStream_t s) {
+  launch_group_gather(fe, x, B, gather_mode, s);
+  switch (fe.n1) {
+    case 3: hx_sf_n<3, 2, false, T>(fe, mt, vj, x, Ycell, B, gather_mode, s); break;
+    case 5: hx_sf_n<5, 2, false, T>(fe, mt, vj, x, Ycell, B, gather_mode, s); break;
+    case 6: hx_sf_n<6, 2, false, T>(fe, mt, vj, x, Ycell, B, gather_mode, s); break;
+    default: throw StatusError(5, "tensor-core operand rounding is built for FE orders 2, 4 and 5");
+  }
+}
+void launch_hx_cell_sf_tc(const FeView &fe, const SfMatsT<Tf32Operand> &mt, const double *vj, const double *x,
+                          double *Ycell, int B, int gather_mode, cudaStream_t s) {
+  hx_sf_tc(fe, mt, vj, x, Ycell, B, gather_mode, s);
+}
+void launch_hx_cell_sf_tc(const FeView &fe, const SfMatsT<Bf16Operand> &mt, const double *vj, const double *x,
+                          double *Ycell, int B, int gather_mode, cudaStream_t s) {
+  hx_sf_tc(fe, mt, vj, x, Ycell, B, gather_mode, s);
 }
 
 void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell,
@@ -2068,6 +2067,28 @@ void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, con
     return;
   }
   hx_sf_dispatch<1>(fe, mt, vj, x, Ycell, B, gather_mode, s);
+}
+
+__global__ void transpose_kernel(const double *__restrict__ a, double *__restrict__ out, int64_t rows,
+                                 int64_t cols) {
+  __shared__ double t[32][33];
+  const int64_t r0 = (int64_t)blockIdx.y * 32, c0 = (int64_t)blockIdx.x * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int64_t r = r0 + i, c = c0 + threadIdx.x;
+    if (r < rows && c < cols) t[i][threadIdx.x] = a[r * cols + c];
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int64_t c = c0 + i, r = r0 + threadIdx.x;
+    if (r < rows && c < cols) out[c * rows + r] = t[threadIdx.x][i];
+  }
+}
+
+void launch_transpose(const double *a, double *out, int64_t rows, int64_t cols, cudaStream_t s) {
+  if (rows * cols == 0) return;
+  const dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
+  transpose_kernel<<<grid, dim3(32, 8), 0, s>>>(a, out, rows, cols);
+  INVDFT_LAUNCH_CHECK();
 }
 
 __global__ void mul_kernel(const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ out,
@@ -2166,7 +2187,7 @@ static AsmBulkShape asm_bulk_shape(const FeView &fe, int B) {
   sh.TR = std::max(16, std::min(256, 1024 / B)) & ~3;
   sh.cap = 2 * sh.TR;
   const size_t seg_n = (size_t)sh.cap * B + 2, blk = (size_t)sh.TR * B;
-  const size_t stage = 8 * (seg_n + 2 * blk + sh.TR) + 4 * 2 * ((size_t)sh.TR + 4);
+  const size_t stage = 8 * (seg_n + 2 * blk + sh.TR) + 4 * ((size_t)sh.TR + 4);
   sh.smem = 2 * ((stage + 127) & ~(size_t)127);
   static int nsm = 0;
   static int occ[257] = {};
@@ -2211,26 +2232,16 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
   if (TR + 1 > kAsmRow * NT || TR * B > kAsmBlk * NT || cap * B > kAsmSeg * NT)
     throw StatusError(5, "assembly tile larger than its staging shares");
   const int nb = (int)((fe.nnodes + TR - 1) / TR);   // one tile of TR nodes per CTA
-  if (fe.nhang > 0) {
-    hanging_sum_kernel<<<ceil_div((int64_t)fe.nhang * B, NT), NT, 0, s>>>(fe, Ycell, B);
-    INVDFT_LAUNCH_CHECK();
-  }
-  if (fe.nmast > 0 && B <= kWarpGroupMaxB && group_warp_enabled()) {
-    group_partial_warp_kernel<<<ceil_div(fe.ngroup_h, NT / 32), NT, 0, s>>>(fe, B);
-    INVDFT_LAUNCH_CHECK();
-    master_sum_kernel<<<ceil_div((int64_t)fe.nmast * B, NT), NT, 0, s>>>(fe, B);
-    INVDFT_LAUNCH_CHECK();
-  } else if (fe.nmast > 0) {
-    const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnr, 1) * (B + std::max(fe.g_maxnm, 1)),
-                                           fe.g_stage);
+  if (fe.nmast > 0) {
+    const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnr, 1) * B, fe.g_stage);
     static bool attr = false;
     if (!attr) {
       INVDFT_CUDA(cudaFuncSetAttribute(group_partial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
       attr = true;
     }
-    group_partial_kernel<<<fe.ngroup_h, NT, sizeof(double) * (size_t)cap, s>>>(fe, B, cap);
+    group_partial_kernel<<<fe.ngroup_h, NT, sizeof(double) * (size_t)cap, s>>>(fe, Ycell, B, cap);
     INVDFT_LAUNCH_CHECK();
-    master_sum_kernel<<<ceil_div((int64_t)fe.nmast * B, NT), NT, 0, s>>>(fe, B);
+    master_sum_kernel<<<ceil_div((int64_t)fe.nmast * B, NT), NT, 0, s>>>(fe, B, const_cast<double *>(Ycell));
     INVDFT_LAUNCH_CHECK();
   }
   // one tile per CTA by default; INVDFT_ASM_KERNEL=bulk selects the
@@ -2240,7 +2251,7 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
     return v && std::string(v) == "bulk";
   }();
   const bool bulk_ok = want_bulk && aligned16(Ycell) && aligned16(fe.dptr) &&
-                       aligned16(fe.midx) && aligned16(fe.inv_sqrt_mass) && (!epi.in || aligned16(epi.in)) &&
+                       aligned16(fe.inv_sqrt_mass) && (!epi.in || aligned16(epi.in)) &&
                        (!epi.prev || aligned16(epi.prev));
   if (bulk_ok) {
     const AsmBulkShape sh = asm_bulk_shape(fe, B);
@@ -2248,10 +2259,10 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
     INVDFT_LAUNCH_CHECK();
     return sh.grid;
   }
-  const size_t smem = sizeof(double) * ((size_t)cap * B + 2 * (size_t)TR * B + TR) + sizeof(int) * (2 * TR + 1);
+  const size_t smem = sizeof(double) * ((size_t)cap * B + 2 * (size_t)TR * B + TR) + sizeof(int) * (TR + 1);
   hx_assemble_tile_kernel<<<nb, NT, smem, s>>>(fe, Ycell, out, B, epi, TR, cap);
   INVDFT_LAUNCH_CHECK();
-  return nb;
+  return (epi.kind == AsmEpilogue::MINRES && epi.dot_ticket) ? 0 : nb;
 }
 
 void launch_scale_rows(const double *d, const double *x, double *y, int64_t n, int B, cudaStream_t s) {

@@ -25,13 +25,19 @@ struct FeView {
   // slots after those, are summed per hanging node into z and reach their
   // masters through the constraint groups below.
   const int *slot_of;       // [nc*nd]
+  // the Lowdin gather map and the slot map transposed, [nd][nc]: for blocks
+  // narrower than 16 columns a CTA of the matrix-free kernel holds several
+  // cells, whose entries for one local index are then contiguous
+  const int *cell_map_t;
+  const int *slot_of_t;
+  // the matrix-free kernel's row-major gather map: node, or -(1 + row of hvg)
+  // for a constrained entry (cell_map_t is its transpose)
+  const int *cell_map_sf;
   const int *dptr;          // [nnodes+1]
   const int *zptr;          // [nhang+1] slot ranges of the hanging nodes' rows
   int nhang;
-  double *z;                // [nhang][B] scratch: summed rows of each hanging node
-  const int *midx;          // [nnodes+8] compact master index of a node (-1: no hanging contributions)
   int nmast;
-  double *mz;               // [nmast][B] scratch: hanging contributions summed per master
+  const int *mslot;         // [nmast] the last slot of each master's range: its summed hanging contributions
   // constraint rows grouped by identical (ordered) master lists: group g owns
   // rows g_rows[g_rptr[g] .. g_rptr[g+1]) (hanging indices g_hrow, -1 for
   // Dirichlet rows), whose masters are cons_masters[g_m0[g] ..][0, g_nm[g]);
@@ -41,13 +47,14 @@ struct FeView {
   int ngroup, ngroup_h, g_maxnm, g_maxnr;
   int g_stage;              // shared staging per group, doubles; larger groups read global memory
   const int *g_rptr, *g_rows, *g_hrow, *g_m0, *g_nm, *g_poff;
-  // the weights of group g's rows, [row q][master t] contiguous from g_woff[g]:
-  // Lowdin-scaled (gw, for the gather) and plain (w, for the transpose)
+  // the plain weights of group g's rows from g_woff[g]: [row q][master t]
+  // (g_w, for the transpose) and [t][q] (g_wt, for the gather); groups with
+  // identical weight blocks share one copy
   const int64_t *g_woff;
-  const double *g_gw, *g_w;
+  const double *g_w, *g_wt;
   const int *mp_ptr, *mp_idx;
   double *gpart;            // [npairs][B] scratch: per (group, master) partial sums
-  double *hvg;              // [ncons][B] scratch: Lowdin-gathered values of the constrained rows
+  double *hvg;              // [nhang+1][B] scratch: Lowdin-gathered hanging rows, then a zero row
   int *err;                 // device error word (bounded waits that gave up)
   const double *inv_sqrt_mass, *sqrt_mass;
 };
@@ -104,7 +111,31 @@ template <typename T> struct SfMatsT {
   }
 };
 using SfMats = SfMatsT<double>;
-// matrix-free variant: vj [nc][nq] = v_KS * JxW at the parent quadrature points;
+
+// FP32 arithmetic whose products take their operands rounded to the input
+// format of a tensor-core MMA: M = 1 TF32 (cvt.rna.tf32.f32, 10-bit mantissa),
+// M = 2 BF16 (round to nearest even, 7-bit mantissa).  The 1D operator
+// applications (the GEMM-shaped part of the cell product) round both operands
+// and accumulate in FP32, as tcgen05.mma kind::tf32 / kind::f16 with an FP32
+// accumulator do; sums, the weights and the potential product (the element-wise
+// epilogue of such a kernel) stay plain FP32.  It measures what those tensor-core
+// products would do to the filter's convergence, at FP32 speed.
+template <int M> struct TcOperand {
+  float v;
+  TcOperand() = default;
+  __host__ __device__ constexpr TcOperand(float x) : v(x) {}
+  __host__ __device__ constexpr TcOperand(double x) : v(float(x)) {}
+  __host__ __device__ constexpr TcOperand(int x) : v(float(x)) {}
+  __host__ __device__ explicit operator double() const { return v; }
+  __host__ __device__ TcOperand &operator*=(TcOperand o) { v *= o.v; return *this; }
+};
+template <int M> __host__ __device__ inline TcOperand<M> operator+(TcOperand<M> a, TcOperand<M> b) { return a.v + b.v; }
+template <int M> __host__ __device__ inline TcOperand<M> operator-(TcOperand<M> a, TcOperand<M> b) { return a.v - b.v; }
+template <int M> __host__ __device__ inline TcOperand<M> operator*(TcOperand<M> a, TcOperand<M> b) { return a.v * b.v; }
+using Tf32Operand = TcOperand<1>;
+using Bf16Operand = TcOperand<2>;
+// matrix-free variant: vj = v_KS * JxW at the parent quadrature points, twice:
+// [nc][nq] followed by its transpose [nq][nc] (read by blocks narrower than 16);
 // tune 0: one CTA per SM allowed the registers it wants, 1: two CTAs per SM,
 // 2: two CTAs per SM with the derivative lines held in shared memory (order 5)
 void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell,
@@ -113,6 +144,14 @@ void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, con
 // low rungs of the mixed-precision Chebyshev ladder
 void launch_hx_cell_sf_f32(const FeView &fe, const SfMatsT<float> &mt, const double *vj, const double *x,
                            double *Ycell, int B, int gather_mode, cudaStream_t s);
+// ... with the 1D operator products on TF32- or BF16-rounded operands (FE orders
+// 2, 4 and 5): the numerics of a tensor-core cell product
+void launch_hx_cell_sf_tc(const FeView &fe, const SfMatsT<Tf32Operand> &mt, const double *vj, const double *x,
+                          double *Ycell, int B, int gather_mode, cudaStream_t s);
+void launch_hx_cell_sf_tc(const FeView &fe, const SfMatsT<Bf16Operand> &mt, const double *vj, const double *x,
+                          double *Ycell, int B, int gather_mode, cudaStream_t s);
+// out[c][q] = a[q][c] (rows x cols -> cols x rows)
+void launch_transpose(const double *a, double *out, int64_t rows, int64_t cols, cudaStream_t s);
 // out[i] = a[i] * b[i]
 void launch_mul(const double *a, const double *b, double *out, int64_t n, cudaStream_t s);
 // out[i] = a x[i] + b y[i] + c z[i] (y, z may be null); out may alias x, y or z
@@ -134,9 +173,12 @@ struct AsmEpilogue {
   const double *psi = nullptr;               // RHS: distributed nodal psi
   const double *minres_coef = nullptr;       // MINRES: beta/oldb per column (0 at itn 1)
   double *dot_partial = nullptr;             // MINRES: per-block column partials of v.y
+  double *dot_out = nullptr;                 // MINRES: if set with dot_ticket, the last CTA reduces the
+  unsigned *dot_ticket = nullptr;            //   partials into dot_out[B] (ticket zero on entry and exit)
 };
 int assemble_blocks(const FeView &fe, int B);  // CTAs of launch_hx_assemble for width B
-// returns the number of CTAs (= MINRES dot partials written)
+// returns the number of CTAs (= MINRES dot partials written), or 0 when the
+// launch has already reduced them into epi.dot_out
 int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B,
                        const AsmEpilogue &epi, int dot_blocks, cudaStream_t s);
 

@@ -135,8 +135,8 @@ void Context::poisson_solve(const double *h_rho, int n_atoms, const double *Z, c
   tmp.upload(pc, stream);
   launch_axpbypcz(bt.p, 4.0 * M_PI, bt.p, 1.0, tmp.p, 0.0, nullptr, nn, stream);
   // the Laplacian: the matrix-free cell product with a zero potential
-  if (vj_zero.n < (size_t)nqt) {
-    vj_zero.alloc((size_t)nqt);
+  if (vj_zero.n < 2 * (size_t)nqt) {   // both layouts of the (zero) potential term
+    vj_zero.alloc(2 * (size_t)nqt);
     vj_zero.zero(stream);
   }
   auto apply = [&](const double *in, double *out) {   // out = 2 Ht0 in

@@ -267,6 +267,30 @@ def test_mixed_precision_ladder_reaches_fp64_accuracy(name, variant, monkeypatch
     assert rel(f_g, f_o) < 1e-6
 
 
+@pytest.mark.parametrize("operands", ["tf32", "bf16"])
+def test_tensor_core_operand_ladder_recovers_fp64(operands, monkeypatch):
+    """MIXED with the filter's low-rung products on TF32 / BF16-rounded operands
+    (the numerics of a tensor-core cell product): those passes run, the ladder
+    leaves them once the residual stops halving, and the FP64 passes still
+    reach the FP64 oracle: occupied eigenvalues 1e-9 Ha, force 1e-6.  The top
+    state of the block sits at the filter's cutoff next to a state 1.4e-4 Ha
+    away, so which of the two a run converges to depends on its start
+    subspace (both are eigenpairs to the 1e-10 residual); it is not compared."""
+    monkeypatch.setenv("INVDFT_LADDER_OPERANDS", operands)
+    P, fn, orc = _pair("small_lih", precision=1, mixed_residual_floor=1e-4)
+    pot = P.vxc_init.copy()
+    f_g, L_g, st = fn.get_force_vector(pot.copy())
+    f_o, L_o, ost = orc.get_force_vector(pot.copy())
+    assert st["passes_low"] >= 1
+    assert st["max_residual"] <= 1e-10
+    e, occ, _ = fn.eigen()
+    occupied = np.asarray(occ) > 1e-8
+    assert occupied.sum() >= 2 and not occupied[-1]
+    assert np.max(np.abs(e[occupied] - ost.eigenvalues[occupied])) < 1e-9
+    assert abs(L_g - L_o) <= 1e-8 * abs(L_o)
+    assert rel(f_g, f_o) < 1e-6
+
+
 @pytest.mark.parametrize("name", ["small_lih", "tiny_h2_p5", "tiny_h2_p4"])
 def test_sf_launch_shapes_are_bitwise_identical(name, monkeypatch):
     """The matrix-free kernel's launch shapes (one or two CTAs per SM,

@@ -1,5 +1,6 @@
 // Shared device/host utilities of the invDFT B200 library.
 #pragma once
+#include <utility>
 
 #include <cuda_runtime.h>
 #include <atomic>
@@ -70,6 +71,11 @@ template <typename T> struct DevBuf {
     }
   }
   void ensure(size_t count) { if (count > n) alloc(count); }
+  // exchange the allocations of two buffers (pointer and size)
+  void swap(DevBuf &o) noexcept {
+    std::swap(p, o.p);
+    std::swap(n, o.n);
+  }
   void release() {
     if (p) {
       cudaFree(p);

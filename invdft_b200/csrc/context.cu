@@ -667,7 +667,10 @@ int Context::sf_shape(const double *d_x, int Bw) {
   std::vector<int> cand = {0};
   if (n1 <= 6) cand.push_back(1);
   if (n1 == 6) cand.push_back(2);
-  if (n1 == 5 || n1 == 6) cand.push_back(3);
+  if (n1 == 5 || n1 == 6) {
+    cand.push_back(3);
+    cand.push_back(4);
+  }
   if (cand.size() == 1) return t = 0;
   cudaEvent_t a, b;
   INVDFT_CUDA(cudaEventCreate(&a));
@@ -1372,8 +1375,7 @@ void Context::minres_core(const double *d_rhs, double *d_x, double tol, int maxi
       gather_columns_kernel<<<ceil_div((int64_t)nn * Bn, 256), 256, 0, stream>>>(V->p, Bc, d_idx.p, m_tmp.p, Bn, nn);
       INVDFT_LAUNCH_CHECK();
       count_launch();
-      std::swap(V->p, m_tmp.p);
-      std::swap(V->n, m_tmp.n);
+      V->swap(m_tmp);
     }
     std::vector<double> hs2(16 * 64, 0.0);
     std::vector<int> hf2(3 * 64, 0);
@@ -1456,9 +1458,13 @@ void Context::minres_core(const double *d_rhs, double *d_x, double tol, int maxi
     n_hx_cols += Bc;
     width_iters[Bc]++;
     if (minres_fused) {
-      launch_minres_update1_fused(m_r1.p, m_r2.p, m_y.p, m_yn.p, diagA.p, st, nn, Bc, partial.p, nblocks_red,
+      launch_minres_update1_fused(m_r2.p, m_yn.p, m_y.p, diagA.p, st, nn, Bc, partial.p, nblocks_red,
                                   m_ticket.p, stream);
+      // (r1, r2, yn) <- (r2, yn, r1): the new r2 was written over yn, r1 is free
+      m_r1.swap(m_r2);
+      m_r2.swap(m_yn);
       launch_minres_update2v(m_xc.p, m_w.p, m_w2.p, m_v.p, m_y.p, st, nn, Bc, stream);
+      m_w.swap(m_w2);   // the new w was written over w2
     } else {
       launch_minres_update1(m_r1.p, m_r2.p, m_y.p, m_yn.p, diagA.p, st, nn, Bc, partial.p, nblocks_red, stream);
       launch_minres_scalars(st, Bc, itn, stream);
@@ -1523,7 +1529,7 @@ void Context::kernel_probe() {
       m_ticket.zero(stream);
     }
     m_v.ensure((size_t)nn * N);
-    launch_minres_update1_fused(m_r1.p, m_r2.p, m_y.p, m_b.p, diagA.p, st, nn, N, partial.p, nblocks_red,
+    launch_minres_update1_fused(m_r2.p, m_b.p, m_y.p, diagA.p, st, nn, N, partial.p, nblocks_red,
                                 m_ticket.p, stream);
     launch_minres_update2v(m_xc.p, m_w.p, m_w2.p, m_v.p, m_y.p, st, nn, N, stream);
   } else {

@@ -599,6 +599,181 @@ __global__ void __launch_bounds__(16 * N * N, MINB) hx_cell_sf_kernel(FeView fe,
   }
 }
 
+// Two (cell, column) pairs per thread: the same stages as hx_cell_sf_kernel
+// (FP64), with thread (pair couple pp, tensor line L) carrying pairs 2pp and
+// 2pp+1 through every stage.  The pairs sit next to each other in the
+// [point][pair] arrays, so each shared access is one 16-byte load or store for
+// both, and each 1D operator coefficient serves two FMA chains; half the
+// threads, twice the independent work per thread.  When a CTA holds one cell
+// per two or more columns (C >= 2) both pairs share the cell, and its gather
+// indices, potential values and slots are loaded once.  Every value is
+// computed by the same operations in the same order as in hx_cell_sf_kernel,
+// so the results are bitwise identical.
+template <int N, int DIR>
+__device__ __forceinline__ void sf_load2(const double *a, int L, int pp, double (&r0)[N], double (&r1)[N]) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    const double2 v = *reinterpret_cast<const double2 *>(&a[sf_point<N, DIR>(L, k) * 16 + 2 * pp]);
+    r0[k] = v.x;
+    r1[k] = v.y;
+  }
+}
+template <int N, int DIR>
+__device__ __forceinline__ void sf_store2(double *a, int L, int pp, const double (&r0)[N], const double (&r1)[N]) {
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+    *reinterpret_cast<double2 *>(&a[sf_point<N, DIR>(L, k) * 16 + 2 * pp]) = make_double2(r0[k], r1[k]);
+}
+
+template <int N, int MINB>
+__global__ void __launch_bounds__(8 * N * N, MINB) hx_cell_sf2_kernel(FeView fe, SfMats mt, const double *__restrict__ vj,
+                                                                const double *__restrict__ x,
+                                                                double *__restrict__ Ycell, int B, int C, int mode) {
+  constexpr int N2 = N * N, N3 = N2 * N;
+  extern __shared__ __align__(16) unsigned char sf_smem[];
+  double *A = reinterpret_cast<double *>(sf_smem), *Bs = A + N3 * 16, *Cs = A + 2 * N3 * 16;
+  const int pp = threadIdx.x & 7, L = threadIdx.x >> 3;
+  const int G = 16 / C;
+  const bool trn = G > 1, same = C >= 2;
+  int64_t e[2];
+  int bc[2];
+  bool act[2];
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    const int p = 2 * pp + u, g = p / C, c = p - g * C;
+    e[u] = (int64_t)blockIdx.x * G + g;
+    bc[u] = blockIdx.y * C + c;
+    act[u] = e[u] < fe.nc && bc[u] < B;
+  }
+  auto at = [&](int u, int l) -> int64_t { return trn ? (int64_t)l * fe.nc + e[u] : e[u] * N3 + l; };
+  const double *vjv = trn ? vj + fe.nc * N3 : vj;
+  double wa = 0.0, wb = 0.0;
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    if (L % N == k) wa = mt.w[k];
+    if (L / N == k) wb = mt.w[k];
+  }
+  double f[2];
+#pragma unroll
+  for (int u = 0; u < 2; ++u) f[u] = sf_mul(sf_mul(act[u] ? 0.5 * fe.cell_h[e[u]] : 0.0, wa), wb);
+  double r[2][N], s[2][N], gx[2][N];
+  {
+    int m[2][N];
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        const int l = L + N2 * k;
+        if (u == 1 && same) {
+          m[1][k] = act[1] ? m[0][k] : 0;
+        } else {
+          m[u][k] = act[u] ? (mode == GATHER_PLAIN ? fe.cell_nodes[e[u] * N3 + l]
+                                                   : (trn ? fe.cell_map_t : fe.cell_map_sf)[at(u, l)])
+                           : 0;
+        }
+      }
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        const bool direct = act[u] && m[u][k] >= 0;
+        const double xv = direct ? x[(int64_t)m[u][k] * B + bc[u]] : 0.0;
+        const double sc = (direct && mode != GATHER_PLAIN) ? fe.inv_sqrt_mass[m[u][k]] : 1.0;
+        r[u][k] = __dmul_rn(xv, sc);
+      }
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int k = 0; k < N; ++k)
+        if (act[u] && m[u][k] < 0) r[u][k] = fe.hvg[(int64_t)(-m[u][k] - 1) * B + bc[u]];
+  }
+#pragma unroll
+  for (int u = 0; u < 2; ++u) sf_phi<N>(mt, r[u], s[u]);
+  sf_store2<N, 2>(A, L, pp, s[0], s[1]);
+  __syncthreads();
+  sf_load2<N, 1>(A, L, pp, r[0], r[1]);   // phi along y
+#pragma unroll
+  for (int u = 0; u < 2; ++u) sf_phi<N>(mt, r[u], s[u]);
+  sf_store2<N, 1>(Bs, L, pp, s[0], s[1]);
+  __syncthreads();
+  sf_load2<N, 0>(Bs, L, pp, r[0], r[1]);  // phi along x: Gauss-point values, then d/dx
+#pragma unroll
+  for (int u = 0; u < 2; ++u) sf_phi<N>(mt, r[u], s[u]);
+  sf_store2<N, 0>(A, L, pp, s[0], s[1]);
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    sf_dq<N>(mt, s[u], gx[u]);
+#pragma unroll
+    for (int q = 0; q < N; ++q) gx[u][q] = sf_mul(gx[u][q], sf_mul(f[u], mt.w[q]));
+  }
+  __syncthreads();
+  sf_load2<N, 1>(A, L, pp, r[0], r[1]);   // d/dy, weighted, kept for the y back pass
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    sf_dq<N>(mt, r[u], s[u]);
+#pragma unroll
+    for (int q = 0; q < N; ++q) s[u][q] = sf_mul(s[u][q], sf_mul(f[u], mt.w[q]));
+  }
+  sf_store2<N, 1>(Cs, L, pp, s[0], s[1]);
+  {
+    double v[2][N];
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int k = 0; k < N; ++k)
+        v[u][k] = (u == 1 && same) ? (act[1] ? v[0][k] : 0.0) : (act[u] ? vjv[at(u, L + N2 * k)] : 0.0);
+    sf_load2<N, 2>(A, L, pp, r[0], r[1]); // d/dz, the z back pass and the potential term
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      sf_dq<N>(mt, r[u], s[u]);
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        s[u][q] = sf_mul(s[u][q], sf_mul(f[u], mt.w[q]));
+        r[u][q] = sf_mul(r[u][q], v[u][q]);
+      }
+      sf_dqt_add<N>(mt, s[u], r[u]);
+    }
+    sf_store2<N, 2>(Bs, L, pp, r[0], r[1]);
+  }
+  __syncthreads();
+  sf_load2<N, 1>(Bs, L, pp, r[0], r[1]);  // y back pass of the derivative term
+  sf_load2<N, 1>(Cs, L, pp, s[0], s[1]);
+#pragma unroll
+  for (int u = 0; u < 2; ++u) sf_dqt_add<N>(mt, s[u], r[u]);
+  sf_store2<N, 1>(A, L, pp, r[0], r[1]);
+  __syncthreads();
+  sf_load2<N, 0>(A, L, pp, r[0], r[1]);   // x back pass, then phi^T along x
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    sf_dqt_add<N>(mt, gx[u], r[u]);
+    sf_phit<N>(mt, r[u], s[u]);
+  }
+  sf_store2<N, 0>(Bs, L, pp, s[0], s[1]);
+  __syncthreads();
+  sf_load2<N, 1>(Bs, L, pp, r[0], r[1]);  // phi^T along y
+#pragma unroll
+  for (int u = 0; u < 2; ++u) sf_phit<N>(mt, r[u], s[u]);
+  sf_store2<N, 1>(A, L, pp, s[0], s[1]);
+  __syncthreads();
+  sf_load2<N, 2>(A, L, pp, r[0], r[1]);   // phi^T along z, straight to the cell-result slots
+#pragma unroll
+  for (int u = 0; u < 2; ++u) sf_phit<N>(mt, r[u], s[u]);
+  int sl[2][N];
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+      sl[u][k] = (u == 1 && same) ? sl[0][k]
+                                  : (act[u] ? (trn ? fe.slot_of_t : fe.slot_of)[at(u, L + N2 * k)] : -1);
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+    if (act[u]) {
+#pragma unroll
+      for (int k = 0; k < N; ++k)
+        if (sl[u][k] >= 0) Ycell[(int64_t)sl[u][k] * B + bc[u]] = s[u][k];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // HX, part 1, bulk-asynchronous variant.  Persistent CTAs walk their cells;
 // thread 0 streams contiguous column panels of H_e (PW columns x ldh doubles)
@@ -1086,12 +1261,12 @@ __device__ __forceinline__ double hanging_row_sum(const FeView &fe, const double
 // master) partials into the master's last slot.  Both in a fixed order.
 __global__ void __launch_bounds__(NT) group_partial_kernel(FeView fe, const double *__restrict__ Ycell, int B,
                                                            int cap) {
-  extern __shared__ double sp[];   // zr [nr][B]
+  extern __shared__ double sp[];   // zr [nr][B] | wm [nr][nm]
   const int g = blockIdx.x;
   const int nm = fe.g_nm[g], rp0 = fe.g_rptr[g], nr = fe.g_rptr[g + 1] - rp0;
   const int64_t po = fe.g_poff[g];
   const double *w = fe.g_w + fe.g_woff[g];
-  if ((int64_t)nr * B > cap) {   // too large to stage: z summed per use from the cell results
+  if ((int64_t)nr * (B + nm) > cap) {   // too large to stage: z summed per use from the cell results
     for (int i = threadIdx.x; i < nm * B; i += blockDim.x) {
       const int t = i / B, j = i - t * B;
       double acc = 0.0;
@@ -1100,16 +1275,17 @@ __global__ void __launch_bounds__(NT) group_partial_kernel(FeView fe, const doub
     }
     return;
   }
-  double *zr = sp;
+  double *zr = sp, *wm = sp + (size_t)nr * B;
   for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
     const int q = i / B, j = i - q * B;
     zr[i] = hanging_row_sum(fe, Ycell, fe.g_hrow[rp0 + q], j, B);
   }
+  for (int i = threadIdx.x; i < nr * nm; i += blockDim.x) wm[i] = w[i];
   __syncthreads();
   for (int i = threadIdx.x; i < nm * B; i += blockDim.x) {
     const int t = i / B, j = i - t * B;
     double acc = 0.0;
-    for (int q = 0; q < nr; ++q) acc = fma(w[q * nm + t], zr[q * B + j], acc);
+    for (int q = 0; q < nr; ++q) acc = fma(wm[q * nm + t], zr[q * B + j], acc);
     fe.gpart[(po + t) * B + j] = acc;
   }
 }
@@ -1567,9 +1743,9 @@ __global__ void minres_scalars_kernel(MinresState st, int B) {
 // of all CTAs -- one warp per column, lanes over the CTAs in a fixed order --
 // into beta2 and runs the scalars; it then resets the ticket.  The sum order
 // does not depend on which CTA is last, so results are reproducible.
-__global__ void __launch_bounds__(NT) minres_update1_fused_kernel(double *__restrict__ r1, double *__restrict__ r2,
+__global__ void __launch_bounds__(NT) minres_update1_fused_kernel(const double *__restrict__ r2,
+                                                                  double *__restrict__ yn,
                                                                   double *__restrict__ y,
-                                                                  const double *__restrict__ yn,
                                                                   const double *__restrict__ diagA, MinresState st,
                                                                   int64_t n, int B, int64_t rows_per_block,
                                                                   double *__restrict__ partial,
@@ -1585,11 +1761,9 @@ __global__ void __launch_bounds__(NT) minres_update1_fused_kernel(double *__rest
     const double a = st.alfa[j] / st.beta[j];
     for (int64_t r = r0 + rr; r < r1e; r += RR) {
       const int64_t idx = r * B + j;
-      const double r2o = r2[idx];
-      const double ynv = yn[idx] - a * r2o;
+      const double ynv = yn[idx] - a * r2[idx];
       const double yv = diagA[r] * ynv;
-      r1[idx] = r2o;
-      r2[idx] = ynv;
+      yn[idx] = ynv;   // the new r2
       y[idx] = yv;
       acc = fma(ynv, yv, acc);
     }
@@ -1615,9 +1789,9 @@ __global__ void __launch_bounds__(NT) minres_update1_fused_kernel(double *__rest
 // update2 (w, w2, x of the committed columns) fused with the next iteration's
 // v = y / beta (beta already the new one): each element is read and written by
 // one thread, so v is updated in place after its old value is used.
-__global__ void minres_update2v_kernel(double *__restrict__ x, double *__restrict__ w, double *__restrict__ w2,
-                                       double *__restrict__ v, const double *__restrict__ y, MinresState st,
-                                       int64_t n, int B) {
+__global__ void minres_update2v_kernel(double *__restrict__ x, const double *__restrict__ w,
+                                       double *__restrict__ w2, double *__restrict__ v,
+                                       const double *__restrict__ y, MinresState st, int64_t n, int B) {
   const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (idx >= n * B) return;
   const int b = (int)(idx % B);
@@ -1625,8 +1799,7 @@ __global__ void minres_update2v_kernel(double *__restrict__ x, double *__restric
   if (st.commit[b]) {
     const double wo = w[idx], w2o = w2[idx];
     const double wn = (vo - st.oldeps[b] * w2o - st.delta[b] * wo) * st.denom[b];
-    w2[idx] = wo;
-    w[idx] = wn;
+    w2[idx] = wn;   // the new w; the caller swaps w and w2
     x[idx] = fma(st.phi[b], wn, x[idx]);
   }
   const double bt = st.beta[b];
@@ -1923,14 +2096,14 @@ void launch_hx_cell_dmma_f32(const FeView &fe, const float *H32, const double *x
 // rows; the weights are read from the group's (shared, [master][row]) block.
 __global__ void __launch_bounds__(NT) group_gather_kernel(FeView fe, const double *__restrict__ x, int B,
                                                           int cap) {
-  extern __shared__ double sg[];   // xm [nm][B]
+  extern __shared__ double sg[];   // xm [nm][B] | wt [nm][nr]
   const int g = blockIdx.x;
   if (g == 0 && threadIdx.x < B) fe.hvg[(int64_t)fe.nhang * B + threadIdx.x] = 0.0;
   if (g >= fe.ngroup_h) return;   // the launch with no hanging group: the zero row only
   const int nm = fe.g_nm[g], m0 = fe.g_m0[g];
   const int rp0 = fe.g_rptr[g], nr = fe.g_rptr[g + 1] - rp0;
   const double *wt = fe.g_wt + fe.g_woff[g];
-  if ((int64_t)nm * B > cap) {
+  if ((int64_t)nm * (B + nr) > cap) {
     // a group too large for the shared staging (rows with hundreds of masters
     // after constraint closure): the same sums, read from global memory
     for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
@@ -1944,16 +2117,18 @@ __global__ void __launch_bounds__(NT) group_gather_kernel(FeView fe, const doubl
     }
     return;
   }
+  double *ws = sg + (size_t)nm * B;
   for (int i = threadIdx.x; i < nm * B; i += blockDim.x) {
     const int t = i / B, j = i - t * B;
     const int mt = fe.cons_masters[m0 + t];
     sg[i] = __dmul_rn(x[(int64_t)mt * B + j], fe.inv_sqrt_mass[mt]);
   }
+  for (int i = threadIdx.x; i < nm * nr; i += blockDim.x) ws[i] = wt[i];
   __syncthreads();
   for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
     const int q = i / B, j = i - q * B;
     double v = 0.0;
-    for (int t = 0; t < nm; ++t) v = fma(wt[t * nr + q], sg[t * B + j], v);
+    for (int t = 0; t < nm; ++t) v = fma(ws[t * nr + q], sg[t * B + j], v);
     fe.hvg[(int64_t)fe.g_hrow[rp0 + q] * B + j] = v;
   }
 }
@@ -1978,6 +2153,25 @@ static void hx_sf_n(const FeView &fe, const SfMatsT<T> &mt, const double *vj, co
   INVDFT_LAUNCH_CHECK();
 }
 
+template <int N, int MINB>
+static void hx_sf2_n(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell, int B,
+                     int mode, cudaStream_t s) {
+  constexpr int threads = 8 * N * N;
+  const size_t smem = sizeof(double) * 3 * (size_t)N * N * N * 16;
+  static bool attr = false;
+  if (!attr) {
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_cell_sf2_kernel<N, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    attr = true;
+  }
+  int C = 1;
+  while (C < B && C < 16) C <<= 1;
+  const int G = 16 / C;
+  const dim3 grid((unsigned)((fe.nc + G - 1) / G), (unsigned)((B + C - 1) / C));
+  hx_cell_sf2_kernel<N, MINB><<<grid, threads, smem, s>>>(fe, mt, vj, x, Ycell, B, C, mode);
+  INVDFT_LAUNCH_CHECK();
+}
+
 template <int MINB>
 static void hx_sf_dispatch(const FeView &fe, const SfMats &mt, const double *vj, const double *x, double *Ycell,
                            int B, int mode, cudaStream_t s) {
@@ -1996,7 +2190,7 @@ static void hx_sf_dispatch(const FeView &fe, const SfMats &mt, const double *vj,
 static void launch_group_gather(const FeView &fe, const double *x, int B, int gather_mode, cudaStream_t s) {
   if (gather_mode != GATHER_PLAIN && fe.ngroup > 0) {
     // staging capacity: the largest group's need, at most fe.g_stage doubles
-    const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnm, 1) * B, fe.g_stage);
+    const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnm, 1) * (B + fe.g_maxnr), fe.g_stage);
     static bool attr = false;
     if (!attr) {
       INVDFT_CUDA(cudaFuncSetAttribute(group_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -2056,6 +2250,14 @@ void launch_hx_cell_sf(const FeView &fe, const SfMats &mt, const double *vj, con
   }
   if (tune == 3 && fe.n1 == 5) {
     hx_sf_n<5, 2, false, double, true>(fe, mt, vj, x, Ycell, B, gather_mode, s);
+    return;
+  }
+  if (tune == 4 && fe.n1 == 6) {   // two pairs per thread, two CTAs per SM
+    hx_sf2_n<6, 2>(fe, mt, vj, x, Ycell, B, gather_mode, s);
+    return;
+  }
+  if (tune == 4 && fe.n1 == 5) {
+    hx_sf2_n<5, 2>(fe, mt, vj, x, Ycell, B, gather_mode, s);
     return;
   }
   if (tune >= 1 && fe.n1 <= 6) {
@@ -2233,7 +2435,8 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
     throw StatusError(5, "assembly tile larger than its staging shares");
   const int nb = (int)((fe.nnodes + TR - 1) / TR);   // one tile of TR nodes per CTA
   if (fe.nmast > 0) {
-    const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnr, 1) * B, fe.g_stage);
+    const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnr, 1) * (B + std::max(fe.g_maxnm, 1)),
+                                           fe.g_stage);
     static bool attr = false;
     if (!attr) {
       INVDFT_CUDA(cudaFuncSetAttribute(group_partial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -2260,9 +2463,14 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
     return sh.grid;
   }
   const size_t smem = sizeof(double) * ((size_t)cap * B + 2 * (size_t)TR * B + TR) + sizeof(int) * (TR + 1);
-  hx_assemble_tile_kernel<<<nb, NT, smem, s>>>(fe, Ycell, out, B, epi, TR, cap);
+  // the last CTA reduces the MINRES dot partials itself only while they are
+  // few (at most 32 per thread); more go to the B-CTA reduction kernel
+  AsmEpilogue e2 = epi;
+  const bool fuse_dot = epi.kind == AsmEpilogue::MINRES && epi.dot_ticket && (int64_t)nb * B <= 32 * NT;
+  if (!fuse_dot) e2.dot_ticket = nullptr;
+  hx_assemble_tile_kernel<<<nb, NT, smem, s>>>(fe, Ycell, out, B, e2, TR, cap);
   INVDFT_LAUNCH_CHECK();
-  return (epi.kind == AsmEpilogue::MINRES && epi.dot_ticket) ? 0 : nb;
+  return fuse_dot ? 0 : nb;
 }
 
 void launch_scale_rows(const double *d, const double *x, double *y, int64_t n, int B, cudaStream_t s) {
@@ -2412,16 +2620,16 @@ void launch_minres_update1(double *r1, double *r2, double *y, const double *yn, 
   launch_reduce_partials(partial, nblocks, B, st.beta2, s);
 }
 
-void launch_minres_update1_fused(double *r1, double *r2, double *y, const double *yn, const double *diagA,
+void launch_minres_update1_fused(const double *r2, double *yn, double *y, const double *diagA,
                                  const MinresState &st, int64_t n, int B, double *partial, int nblocks,
                                  unsigned *ticket, cudaStream_t s) {
   const int64_t rpb = (n + nblocks - 1) / nblocks;
-  minres_update1_fused_kernel<<<nblocks, NT, 0, s>>>(r1, r2, y, yn, diagA, st, n, B, rpb, partial, ticket);
+  minres_update1_fused_kernel<<<nblocks, NT, 0, s>>>(r2, yn, y, diagA, st, n, B, rpb, partial, ticket);
   INVDFT_LAUNCH_CHECK();
 }
 
-void launch_minres_update2v(double *x, double *w, double *w2, double *v, const double *y, const MinresState &st,
-                            int64_t n, int B, cudaStream_t s) {
+void launch_minres_update2v(double *x, const double *w, double *w2, double *v, const double *y,
+                            const MinresState &st, int64_t n, int B, cudaStream_t s) {
   minres_update2v_kernel<<<ceil_div(n * B, NT), NT, 0, s>>>(x, w, w2, v, y, st, n, B);
   INVDFT_LAUNCH_CHECK();
 }

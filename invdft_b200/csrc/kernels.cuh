@@ -242,13 +242,16 @@ void launch_minres_init(const double *b, const double *diagA, double *r1, double
                         int64_t n, int B, double *partial, int nblocks, cudaStream_t s);
 void launch_minres_init_scalars(const MinresState &st, const double *beta1_sq, int B, cudaStream_t s);
 // update1 + the reduction of beta2 + the scalar update in one launch (the last
-// CTA reduces and updates; *ticket must be 0 before, and is 0 after)
-void launch_minres_update1_fused(double *r1, double *r2, double *y, const double *yn, const double *diagA,
+// CTA reduces and updates; *ticket must be 0 before, and is 0 after).  The new
+// r2 = yn - (alfa/beta) r2 is written over yn; the caller then rotates the
+// buffers (r1, r2, yn) <- (r2, yn, r1) instead of copying r2 into r1.
+void launch_minres_update1_fused(const double *r2, double *yn, double *y, const double *diagA,
                                  const MinresState &st, int64_t n, int B, double *partial, int nblocks,
                                  unsigned *ticket, cudaStream_t s);
-// update2 + the next iteration's v = y / beta in one launch (v in place)
-void launch_minres_update2v(double *x, double *w, double *w2, double *v, const double *y, const MinresState &st,
-                            int64_t n, int B, cudaStream_t s);
+// update2 + the next iteration's v = y / beta in one launch (v in place).  The
+// new w is written over w2; the caller then swaps the buffers w and w2.
+void launch_minres_update2v(double *x, const double *w, double *w2, double *v, const double *y,
+                            const MinresState &st, int64_t n, int B, cudaStream_t s);
 
 // Child mesh transfers
 struct ChildView {

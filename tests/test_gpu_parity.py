@@ -303,7 +303,7 @@ def test_sf_launch_shapes_are_bitwise_identical(name, monkeypatch):
     else:
         from invdft_b200.problem.system import build_problem
         P = build_problem(name, target_solver="atoms")
-    shapes = ["0", "1"] + (["2"] if P.p == 5 else []) + (["3"] if P.p in (4, 5) else [])
+    shapes = ["0", "1"] + (["2"] if P.p == 5 else []) + (["3", "4"] if P.p in (4, 5) else [])
     out = {}
     for shape in shapes + ["auto"]:
         if shape == "auto":

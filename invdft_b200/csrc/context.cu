@@ -123,20 +123,22 @@ void build_scatter(int64_t nrows, int64_t ncell, int per_cell, const int64_t *ce
 
 // Slot layout of cell results (see FeView): direct slots of free nodes sorted by
 // node then by (cell, local); rows of hanging nodes in slots after those,
-// grouped by hanging node (zptr ranges, summed into z[hanging node] first,
-// then carried to the masters by the constraint groups); Dirichlet rows dropped.
+// grouped by hanging node in hanging-index order (zptr ranges, summed per
+// hanging node and carried to the masters by the constraint groups, whose rows
+// have consecutive hanging indices); Dirichlet rows dropped.
 // Each master of hanging nodes (midx[n] >= 0) owns one more slot, the last of
 // its range, which the master-sum pass fills with the node's pre-summed
 // hanging contributions (mslot[midx[n]]), so that the assembly's sum over the
 // node's contiguous slots already includes them.
 void build_slots(int64_t nrows, int64_t ncell, int per_cell, const int64_t *cell_nodes,
-                 const invdft_constraints &c, const std::vector<int> &midx, std::vector<int> &slot_of,
-                 std::vector<int> &dptr, std::vector<int> &zptr, std::vector<int> &mslot) {
-  std::vector<int64_t> crow(nrows, -1), hidx(c.n_rows, -1);
+                 const invdft_constraints &c, const std::vector<int> &midx, const std::vector<int> &hidx,
+                 std::vector<int> &slot_of, std::vector<int> &dptr, std::vector<int> &zptr,
+                 std::vector<int> &mslot) {
+  // hidx: hanging index of each constraint row with masters (-1: Dirichlet)
+  std::vector<int64_t> crow(nrows, -1);
   for (int64_t r = 0; r < c.n_rows; ++r) crow[c.rows[r]] = r;
   int64_t nh = 0;
-  for (int64_t r = 0; r < c.n_rows; ++r)
-    if (c.ptr[r + 1] > c.ptr[r]) hidx[r] = nh++;
+  for (int64_t r = 0; r < c.n_rows; ++r) nh += hidx[r] >= 0;
   const int64_t tot = ncell * per_cell;
   if (tot > INT32_MAX) throw StatusError(INVDFT_BAD_ARG, "more than 2^31 cell rows");
   std::vector<int64_t> cnt(nrows + 1, 0), zcnt(nh + 1, 0);
@@ -176,6 +178,7 @@ void build_slots(int64_t nrows, int64_t ncell, int per_cell, const int64_t *cell
 // compact index and list of partial rows, in group order.
 struct ConsGroups {
   std::vector<int> rptr{0}, rows, hrow, m0, nm, poff, midx, mp_ptr{0}, mp_idx;
+  std::vector<int> hidx;         // per constraint row: hanging index (group order), -1 for Dirichlet rows
   std::vector<int64_t> woff;     // start of each group's [row][master] weight block
   int ngroup = 0, ngroup_h = 0, maxnm = 0, maxnr = 0, nmast = 0, npairs = 0;
   int64_t nw = 0;
@@ -183,10 +186,13 @@ struct ConsGroups {
 
 ConsGroups build_groups(int64_t nrows, const invdft_constraints &c) {
   ConsGroups G;
+  // hanging rows are numbered in the order the groups emit them, so a group's
+  // rows have consecutive hanging indices (and contiguous slots, zptr ranges
+  // and pre-gathered rows)
   std::vector<int> hidx(c.n_rows, -1);
-  int nh = 0;
   for (int64_t r = 0; r < c.n_rows; ++r)
-    if (c.ptr[r + 1] > c.ptr[r]) hidx[r] = nh++;
+    if (c.ptr[r + 1] > c.ptr[r]) hidx[r] = 0;
+  int nh = 0;
   std::map<std::vector<int64_t>, int> key;
   std::vector<std::vector<int>> members;
   for (int64_t r = 0; r < c.n_rows; ++r) {
@@ -202,6 +208,7 @@ ConsGroups build_groups(int64_t nrows, const invdft_constraints &c) {
   auto emit = [&](const std::vector<int> &L, size_t a, size_t b, int m0, int nm) {
     for (size_t q = a; q < b; ++q) {
       G.rows.push_back(L[q]);
+      if (hidx[L[q]] >= 0) hidx[L[q]] = nh++;
       G.hrow.push_back(hidx[L[q]]);
     }
     G.rptr.push_back((int)G.rows.size());
@@ -224,6 +231,7 @@ ConsGroups build_groups(int64_t nrows, const invdft_constraints &c) {
     if (hidx[r] < 0) dir.push_back((int)r);
   for (size_t a = 0; a < dir.size(); a += kGroupRows) emit(dir, a, std::min(dir.size(), a + kGroupRows), 0, 0);
   G.ngroup = (int)G.nm.size();
+  G.hidx = hidx;
   // masters: compact numbering in node order, partial rows in group order
   std::vector<int> cnt(nrows, 0);
   for (int g = 0; g < G.ngroup_h; ++g)
@@ -385,7 +393,7 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   for (int64_t k = 0; k < nmast; ++k) cgw[k] = d->cons_psi.weights[k] * ism[d->cons_psi.masters[k]];
   const ConsGroups G = build_groups(nn, d->cons_psi);
   std::vector<int> slot_of, dptr_h, zptr_h, mslot_h;
-  build_slots(nn, nc, nd, d->cell_nodes, d->cons_psi, G.midx, slot_of, dptr_h, zptr_h, mslot_h);
+  build_slots(nn, nc, nd, d->cell_nodes, d->cons_psi, G.midx, G.hidx, slot_of, dptr_h, zptr_h, mslot_h);
   nhang = (int)zptr_h.size() - 1;
   n_slots = zptr_h.back();
 
@@ -408,8 +416,7 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
     int nh = 0;
     for (int64_t r = 0; r < d->cons_psi.n_rows; ++r) nh += d->cons_psi.ptr[r + 1] > d->cons_psi.ptr[r];
     std::vector<int> hrow_of(d->cons_psi.n_rows);
-    for (int64_t r = 0, h = 0; r < d->cons_psi.n_rows; ++r)
-      hrow_of[r] = d->cons_psi.ptr[r + 1] > d->cons_psi.ptr[r] ? (int)h++ : nh;
+    for (int64_t r = 0; r < d->cons_psi.n_rows; ++r) hrow_of[r] = G.hidx[r] >= 0 ? G.hidx[r] : nh;
     check(nh == nhang, "hanging row count mismatch");
     std::vector<int> msf(cm.size());
     for (size_t t = 0; t < cm.size(); ++t) msf[t] = cm[t] >= 0 ? cm[t] : -(1 + hrow_of[-cm[t] - 1]);

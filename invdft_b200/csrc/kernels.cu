@@ -966,49 +966,69 @@ __device__ void cta_column_sums(const double *partial, int nparts, int B, double
 // M^-1/2 from ism and the epilogue inputs from t_in/t_prev (all tile-local, row
 // stride B for blocks).  Thread (rr, j) handles column j of rows rr, rr+RR, ...
 // in a fixed order.
+template <int KIND>
+__device__ __forceinline__ void assemble_tile_rows_k(const FeView &fe, const double *segp, int64_t a0,
+                                                     const int *dp, const double *ism,
+                                                     const double *t_in, const double *t_prev, int64_t r0, int rows,
+                                                     double *__restrict__ out, int B, const AsmEpilogue &epi,
+                                                     double &dot) {
+  const int RR = NT / B;
+  const int j = threadIdx.x % B, rr = threadIdx.x / B;
+  if (rr >= RR) return;
+  const double *sj = segp + j;
+  for (int lr = rr; lr < rows; lr += RR) {
+    const int64_t n = r0 + lr;
+    const int d0 = dp[lr], d1 = dp[lr + 1];
+    double acc = 0.0;   // a master's hanging contributions are its last slot
+    for (int sl = d0; sl < d1; ++sl) acc += sj[(int64_t)sl * B - a0];
+    acc *= ism[lr];
+    const int64_t idx = n * B + j;
+    const int li = lr * B + j;
+    if constexpr (KIND == AsmEpilogue::STORE) {
+      out[idx] = acc;
+    } else if constexpr (KIND == AsmEpilogue::CHEB) {
+      double v = epi.alpha * (acc - epi.c * t_in[li]);
+      if (epi.prev) v -= epi.beta * t_prev[li];
+      out[idx] = v;
+    } else if constexpr (KIND == AsmEpilogue::VMULT) {
+      out[idx] = acc - epi.eps[j] * t_in[li];
+    } else if constexpr (KIND == AsmEpilogue::RHS) {
+      double v = 0.0;
+      if (d1 > d0 && ism[lr] != 0.0) {
+        double mu = 0.0;
+        for (int k = 0; k < B; ++k) mu = fma(epi.Mu[k * B + j], epi.psi[n * B + k], mu);
+        v = epi.occ4[j] * acc - 2.0 * fe.sqrt_mass[n] * mu;
+      }
+      out[idx] = v;
+    } else {
+      const double vv = t_in[li];
+      const double yn = acc - epi.eps[j] * vv - epi.minres_coef[j] * t_prev[li];
+      out[idx] = yn;
+      dot = fma(vv, yn, dot);
+    }
+  }
+}
+// the same with the epilogue chosen at run time (the bulk-pipelined variant)
 __device__ __forceinline__ void assemble_tile_rows(const FeView &fe, const double *segp, int64_t a0,
                                                    const int *dp, const double *ism,
                                                    const double *t_in, const double *t_prev, int64_t r0, int rows,
                                                    double *__restrict__ out, int B, const AsmEpilogue &epi,
                                                    double &dot) {
-  const int RR = NT / B;
-  const int j = threadIdx.x % B, rr = threadIdx.x / B;
-  if (rr >= RR) return;
-  for (int lr = rr; lr < rows; lr += RR) {
-    const int64_t n = r0 + lr;
-    const int d0 = dp[lr], d1 = dp[lr + 1];
-    double acc = 0.0;   // a master's hanging contributions are its last slot
-    for (int sl = d0; sl < d1; ++sl) acc += segp[(int64_t)sl * B + j - a0];
-    acc *= ism[lr];
-    const int64_t idx = n * B + j;
-    const int li = lr * B + j;
-    switch (epi.kind) {
-      case AsmEpilogue::STORE: out[idx] = acc; break;
-      case AsmEpilogue::CHEB: {
-        double v = epi.alpha * (acc - epi.c * t_in[li]);
-        if (epi.prev) v -= epi.beta * t_prev[li];
-        out[idx] = v;
-        break;
-      }
-      case AsmEpilogue::VMULT: out[idx] = acc - epi.eps[j] * t_in[li]; break;
-      case AsmEpilogue::RHS: {
-        double v = 0.0;
-        if (d1 > d0 && ism[lr] != 0.0) {
-          double mu = 0.0;
-          for (int k = 0; k < B; ++k) mu = fma(epi.Mu[k * B + j], epi.psi[n * B + k], mu);
-          v = epi.occ4[j] * acc - 2.0 * fe.sqrt_mass[n] * mu;
-        }
-        out[idx] = v;
-        break;
-      }
-      case AsmEpilogue::MINRES: {
-        const double vv = t_in[li];
-        const double yn = acc - epi.eps[j] * vv - epi.minres_coef[j] * t_prev[li];
-        out[idx] = yn;
-        dot = fma(vv, yn, dot);
-        break;
-      }
-    }
+  switch (epi.kind) {
+    case AsmEpilogue::STORE:
+      assemble_tile_rows_k<AsmEpilogue::STORE>(fe, segp, a0, dp, ism, t_in, t_prev, r0, rows, out, B, epi, dot);
+      break;
+    case AsmEpilogue::CHEB:
+      assemble_tile_rows_k<AsmEpilogue::CHEB>(fe, segp, a0, dp, ism, t_in, t_prev, r0, rows, out, B, epi, dot);
+      break;
+    case AsmEpilogue::VMULT:
+      assemble_tile_rows_k<AsmEpilogue::VMULT>(fe, segp, a0, dp, ism, t_in, t_prev, r0, rows, out, B, epi, dot);
+      break;
+    case AsmEpilogue::RHS:
+      assemble_tile_rows_k<AsmEpilogue::RHS>(fe, segp, a0, dp, ism, t_in, t_prev, r0, rows, out, B, epi, dot);
+      break;
+    default:
+      assemble_tile_rows_k<AsmEpilogue::MINRES>(fe, segp, a0, dp, ism, t_in, t_prev, r0, rows, out, B, epi, dot);
   }
 }
 
@@ -1024,6 +1044,7 @@ constexpr int kAsmSeg = 8;   // ... of a staged slot segment (cap B = 2 TR B <= 
 // last slot, written by the master-sum pass.  Thread (rr, j) handles column j of nodes r0+rr,
 // r0+rr+RR, ... (fixed order), so the MINRES dot partials are deterministic.
 // ---------------------------------------------------------------------------
+template <int KIND>
 __global__ void __launch_bounds__(NT, 4) hx_assemble_tile_kernel(FeView fe, const double *__restrict__ Ycell,
                                                               double *__restrict__ out, int B, AsmEpilogue epi,
                                                               int TR, int cap_slots) {
@@ -1039,9 +1060,8 @@ __global__ void __launch_bounds__(NT, 4) hx_assemble_tile_kernel(FeView fe, cons
   const int64_t r0 = (int64_t)blockIdx.x * TR;
   // the grid is sized by the caller (ceil(nnodes / TR)), so rows >= 1
   const int rows = (int)max((int64_t)0, min((int64_t)TR, fe.nnodes - r0));
-  const bool need_in = epi.kind == AsmEpilogue::CHEB || epi.kind == AsmEpilogue::VMULT ||
-                       epi.kind == AsmEpilogue::MINRES;
-  const bool need_prev = (epi.kind == AsmEpilogue::CHEB && epi.prev) || epi.kind == AsmEpilogue::MINRES;
+  constexpr bool need_in = KIND == AsmEpilogue::CHEB || KIND == AsmEpilogue::VMULT || KIND == AsmEpilogue::MINRES;
+  const bool need_prev = (KIND == AsmEpilogue::CHEB && epi.prev) || KIND == AsmEpilogue::MINRES;
   // one round of loads: the slot bounds of the tile first, then every staged
   // array into fixed per-thread register shares (the launcher keeps
   // TR*B <= kAsmBlk*NT and 2*TR*B <= kAsmSeg*NT), then all stores
@@ -1088,9 +1108,9 @@ __global__ void __launch_bounds__(NT, 4) hx_assemble_tile_kernel(FeView fe, cons
   }
   __syncthreads();
   double dot = 0.0;
-  assemble_tile_rows(fe, staged ? seg : Ycell, staged ? (int64_t)s0 * B : 0, dp, ism, s_in, s_prev, r0, rows,
-                     out, B, epi, dot);
-  if (epi.kind == AsmEpilogue::MINRES) {
+  assemble_tile_rows_k<KIND>(fe, staged ? seg : Ycell, staged ? (int64_t)s0 * B : 0, dp, ism, s_in, s_prev, r0,
+                             rows, out, B, epi, dot);
+  if constexpr (KIND == AsmEpilogue::MINRES) {
     const int RR = NT / B;
     red[threadIdx.x] = dot;
     __syncthreads();
@@ -1261,16 +1281,18 @@ __device__ __forceinline__ double hanging_row_sum(const FeView &fe, const double
 // master) partials into the master's last slot.  Both in a fixed order.
 __global__ void __launch_bounds__(NT) group_partial_kernel(FeView fe, const double *__restrict__ Ycell, int B,
                                                            int cap) {
-  extern __shared__ double sp[];   // zr [nr][B] | wm [nr][nm]
+  extern __shared__ double sp[];   // zr [nr][B] | wm [nr][nmp] (rows padded to 4 with zeros)
   const int g = blockIdx.x;
   const int nm = fe.g_nm[g], rp0 = fe.g_rptr[g], nr = fe.g_rptr[g + 1] - rp0;
+  const int nmp = (nm + 3) & ~3;
+  const int h0 = fe.g_hrow[rp0];   // the group's rows have consecutive hanging indices
   const int64_t po = fe.g_poff[g];
   const double *w = fe.g_w + fe.g_woff[g];
-  if ((int64_t)nr * (B + nm) > cap) {   // too large to stage: z summed per use from the cell results
+  if ((int64_t)nr * (B + nmp) > cap) {   // too large to stage: z summed per use from the cell results
     for (int i = threadIdx.x; i < nm * B; i += blockDim.x) {
       const int t = i / B, j = i - t * B;
       double acc = 0.0;
-      for (int q = 0; q < nr; ++q) acc = fma(w[q * nm + t], hanging_row_sum(fe, Ycell, fe.g_hrow[rp0 + q], j, B), acc);
+      for (int q = 0; q < nr; ++q) acc = fma(w[q * nm + t], hanging_row_sum(fe, Ycell, (h0 + q), j, B), acc);
       fe.gpart[(po + t) * B + j] = acc;
     }
     return;
@@ -1278,15 +1300,38 @@ __global__ void __launch_bounds__(NT) group_partial_kernel(FeView fe, const doub
   double *zr = sp, *wm = sp + (size_t)nr * B;
   for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
     const int q = i / B, j = i - q * B;
-    zr[i] = hanging_row_sum(fe, Ycell, fe.g_hrow[rp0 + q], j, B);
+    zr[i] = hanging_row_sum(fe, Ycell, (h0 + q), j, B);
   }
-  for (int i = threadIdx.x; i < nr * nm; i += blockDim.x) wm[i] = w[i];
+  for (int i = threadIdx.x; i < nr * nmp; i += blockDim.x) {
+    const int q = i / nmp, t = i - q * nmp;
+    wm[i] = t < nm ? w[q * nm + t] : 0.0;
+  }
   __syncthreads();
-  for (int i = threadIdx.x; i < nm * B; i += blockDim.x) {
-    const int t = i / B, j = i - t * B;
-    double acc = 0.0;
-    for (int q = 0; q < nr; ++q) acc = fma(wm[q * nm + t], zr[q * B + j], acc);
-    fe.gpart[(po + t) * B + j] = acc;
+  if (B >= 8) {
+    // four masters per thread: each staged z value serves four FMA chains
+    for (int i = threadIdx.x; i < (nmp >> 2) * B; i += blockDim.x) {
+      const int t0 = (i / B) << 2, j = i % B;
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      for (int q = 0; q < nr; ++q) {
+        const double z = zr[q * B + j];
+        const double *wr = wm + q * nmp + t0;
+        a0 = fma(wr[0], z, a0);
+        a1 = fma(wr[1], z, a1);
+        a2 = fma(wr[2], z, a2);
+        a3 = fma(wr[3], z, a3);
+      }
+      const double aa[4] = {a0, a1, a2, a3};
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (t0 + u < nm) fe.gpart[(po + t0 + u) * B + j] = aa[u];
+    }
+  } else {
+    for (int i = threadIdx.x; i < nm * B; i += blockDim.x) {
+      const int t = i / B, j = i - t * B;
+      double acc = 0.0;
+      for (int q = 0; q < nr; ++q) acc = fma(wm[q * nmp + t], zr[q * B + j], acc);
+      fe.gpart[(po + t) * B + j] = acc;
+    }
   }
 }
 
@@ -2096,14 +2141,16 @@ void launch_hx_cell_dmma_f32(const FeView &fe, const float *H32, const double *x
 // rows; the weights are read from the group's (shared, [master][row]) block.
 __global__ void __launch_bounds__(NT) group_gather_kernel(FeView fe, const double *__restrict__ x, int B,
                                                           int cap) {
-  extern __shared__ double sg[];   // xm [nm][B] | wt [nm][nr]
+  extern __shared__ double sg[];   // xm [nm][B] | wt [nm][nrp] (rows padded to 4 with zeros)
   const int g = blockIdx.x;
   if (g == 0 && threadIdx.x < B) fe.hvg[(int64_t)fe.nhang * B + threadIdx.x] = 0.0;
   if (g >= fe.ngroup_h) return;   // the launch with no hanging group: the zero row only
   const int nm = fe.g_nm[g], m0 = fe.g_m0[g];
   const int rp0 = fe.g_rptr[g], nr = fe.g_rptr[g + 1] - rp0;
+  const int nrp = (nr + 3) & ~3;
+  const int h0 = fe.g_hrow[rp0];   // the group's rows have consecutive hanging indices
   const double *wt = fe.g_wt + fe.g_woff[g];
-  if ((int64_t)nm * (B + nr) > cap) {
+  if ((int64_t)nm * (B + nrp) > cap) {
     // a group too large for the shared staging (rows with hundreds of masters
     // after constraint closure): the same sums, read from global memory
     for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
@@ -2113,7 +2160,7 @@ __global__ void __launch_bounds__(NT) group_gather_kernel(FeView fe, const doubl
         const int mt = fe.cons_masters[m0 + t];
         v = fma(wt[t * nr + q], __dmul_rn(x[(int64_t)mt * B + j], fe.inv_sqrt_mass[mt]), v);
       }
-      fe.hvg[(int64_t)fe.g_hrow[rp0 + q] * B + j] = v;
+      fe.hvg[(int64_t)(h0 + q) * B + j] = v;
     }
     return;
   }
@@ -2123,13 +2170,36 @@ __global__ void __launch_bounds__(NT) group_gather_kernel(FeView fe, const doubl
     const int mt = fe.cons_masters[m0 + t];
     sg[i] = __dmul_rn(x[(int64_t)mt * B + j], fe.inv_sqrt_mass[mt]);
   }
-  for (int i = threadIdx.x; i < nm * nr; i += blockDim.x) ws[i] = wt[i];
+  for (int i = threadIdx.x; i < nm * nrp; i += blockDim.x) {
+    const int t = i / nrp, q = i - t * nrp;
+    ws[i] = q < nr ? wt[t * nr + q] : 0.0;
+  }
   __syncthreads();
-  for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
-    const int q = i / B, j = i - q * B;
-    double v = 0.0;
-    for (int t = 0; t < nm; ++t) v = fma(ws[t * nr + q], sg[t * B + j], v);
-    fe.hvg[(int64_t)fe.g_hrow[rp0 + q] * B + j] = v;
+  if (B >= 8) {
+    // four rows per thread: each staged master value serves four FMA chains
+    for (int i = threadIdx.x; i < (nrp >> 2) * B; i += blockDim.x) {
+      const int q0 = (i / B) << 2, j = i % B;
+      double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+      for (int t = 0; t < nm; ++t) {
+        const double xs = sg[t * B + j];
+        const double *wr = ws + t * nrp + q0;
+        v0 = fma(wr[0], xs, v0);
+        v1 = fma(wr[1], xs, v1);
+        v2 = fma(wr[2], xs, v2);
+        v3 = fma(wr[3], xs, v3);
+      }
+      const double vv[4] = {v0, v1, v2, v3};
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (q0 + u < nr) fe.hvg[(int64_t)(h0 + q0 + u) * B + j] = vv[u];
+    }
+  } else {
+    for (int i = threadIdx.x; i < nr * B; i += blockDim.x) {
+      const int q = i / B, j = i - q * B;
+      double v = 0.0;
+      for (int t = 0; t < nm; ++t) v = fma(ws[t * nrp + q], sg[t * B + j], v);
+      fe.hvg[(int64_t)(h0 + q) * B + j] = v;
+    }
   }
 }
 
@@ -2190,14 +2260,18 @@ static void hx_sf_dispatch(const FeView &fe, const SfMats &mt, const double *vj,
 static void launch_group_gather(const FeView &fe, const double *x, int B, int gather_mode, cudaStream_t s) {
   if (gather_mode != GATHER_PLAIN && fe.ngroup > 0) {
     // staging capacity: the largest group's need, at most fe.g_stage doubles
-    const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnm, 1) * (B + fe.g_maxnr), fe.g_stage);
+    const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnm, 1) * (B + ((fe.g_maxnr + 3) & ~3)),
+                                           fe.g_stage);
     static bool attr = false;
     if (!attr) {
       INVDFT_CUDA(cudaFuncSetAttribute(group_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
       attr = true;
     }
-    // the hanging groups; block 0 also writes the zero row
-    group_gather_kernel<<<std::max(fe.ngroup_h, 1), NT, sizeof(double) * (size_t)cap, s>>>(fe, x, B, cap);
+    // the hanging groups; block 0 also writes the zero row.  Narrow blocks keep
+    // few threads of a CTA busy, so they get 64-thread CTAs: more of them fit an
+    // SM, and the groups take fewer waves
+    const int threads = B <= 2 ? 64 : NT;
+    group_gather_kernel<<<std::max(fe.ngroup_h, 1), threads, sizeof(double) * (size_t)cap, s>>>(fe, x, B, cap);
     INVDFT_LAUNCH_CHECK();
   }
 }
@@ -2425,8 +2499,16 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
   if (B > NT) throw StatusError(5, "block width above 256");
   static bool attr = false;
   if (!attr) {
-    INVDFT_CUDA(cudaFuncSetAttribute(hx_assemble_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     100 * 1024));
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_assemble_tile_kernel<AsmEpilogue::STORE>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_assemble_tile_kernel<AsmEpilogue::CHEB>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_assemble_tile_kernel<AsmEpilogue::VMULT>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_assemble_tile_kernel<AsmEpilogue::RHS>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    INVDFT_CUDA(cudaFuncSetAttribute(hx_assemble_tile_kernel<AsmEpilogue::MINRES>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     attr = true;
   }
   int TR, cap;
@@ -2435,14 +2517,14 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
     throw StatusError(5, "assembly tile larger than its staging shares");
   const int nb = (int)((fe.nnodes + TR - 1) / TR);   // one tile of TR nodes per CTA
   if (fe.nmast > 0) {
-    const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnr, 1) * (B + std::max(fe.g_maxnm, 1)),
+    const int cap = (int)std::min<int64_t>((int64_t)std::max(fe.g_maxnr, 1) * (B + ((std::max(fe.g_maxnm, 1) + 3) & ~3)),
                                            fe.g_stage);
     static bool attr = false;
     if (!attr) {
       INVDFT_CUDA(cudaFuncSetAttribute(group_partial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
       attr = true;
     }
-    group_partial_kernel<<<fe.ngroup_h, NT, sizeof(double) * (size_t)cap, s>>>(fe, Ycell, B, cap);
+    group_partial_kernel<<<fe.ngroup_h, B <= 2 ? 64 : NT, sizeof(double) * (size_t)cap, s>>>(fe, Ycell, B, cap);
     INVDFT_LAUNCH_CHECK();
     master_sum_kernel<<<ceil_div((int64_t)fe.nmast * B, NT), NT, 0, s>>>(fe, B, const_cast<double *>(Ycell));
     INVDFT_LAUNCH_CHECK();
@@ -2468,7 +2550,22 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
   AsmEpilogue e2 = epi;
   const bool fuse_dot = epi.kind == AsmEpilogue::MINRES && epi.dot_ticket && (int64_t)nb * B <= 32 * NT;
   if (!fuse_dot) e2.dot_ticket = nullptr;
-  hx_assemble_tile_kernel<<<nb, NT, smem, s>>>(fe, Ycell, out, B, e2, TR, cap);
+  switch (epi.kind) {
+    case AsmEpilogue::STORE:
+      hx_assemble_tile_kernel<AsmEpilogue::STORE><<<nb, NT, smem, s>>>(fe, Ycell, out, B, e2, TR, cap);
+      break;
+    case AsmEpilogue::CHEB:
+      hx_assemble_tile_kernel<AsmEpilogue::CHEB><<<nb, NT, smem, s>>>(fe, Ycell, out, B, e2, TR, cap);
+      break;
+    case AsmEpilogue::VMULT:
+      hx_assemble_tile_kernel<AsmEpilogue::VMULT><<<nb, NT, smem, s>>>(fe, Ycell, out, B, e2, TR, cap);
+      break;
+    case AsmEpilogue::RHS:
+      hx_assemble_tile_kernel<AsmEpilogue::RHS><<<nb, NT, smem, s>>>(fe, Ycell, out, B, e2, TR, cap);
+      break;
+    default:
+      hx_assemble_tile_kernel<AsmEpilogue::MINRES><<<nb, NT, smem, s>>>(fe, Ycell, out, B, e2, TR, cap);
+  }
   INVDFT_LAUNCH_CHECK();
   return fuse_dot ? 0 : nb;
 }

@@ -1804,7 +1804,26 @@ __global__ void __launch_bounds__(NT) minres_update1_fused_kernel(const double *
   double acc = 0.0;
   if (rr < RR && st.active[j]) {
     const double a = st.alfa[j] / st.beta[j];
-    for (int64_t r = r0 + rr; r < r1e; r += RR) {
+    int64_t r = r0 + rr;
+    // four rows in flight per thread (their loads issue together); the dot
+    // accumulates in row order, as the one-row loop below does
+    for (; r + 3 * RR < r1e; r += 4 * RR) {
+      double ynv[4], yv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int64_t ru = r + u * RR, idx = ru * B + j;
+        ynv[u] = yn[idx] - a * r2[idx];
+        yv[u] = diagA[ru] * ynv[u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int64_t idx = (r + u * RR) * B + j;
+        yn[idx] = ynv[u];   // the new r2
+        y[idx] = yv[u];
+        acc = fma(ynv[u], yv[u], acc);
+      }
+    }
+    for (; r < r1e; r += RR) {
       const int64_t idx = r * B + j;
       const double ynv = yn[idx] - a * r2[idx];
       const double yv = diagA[r] * ynv;
@@ -2267,11 +2286,9 @@ static void launch_group_gather(const FeView &fe, const double *x, int B, int ga
       INVDFT_CUDA(cudaFuncSetAttribute(group_gather_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
       attr = true;
     }
-    // the hanging groups; block 0 also writes the zero row.  Narrow blocks keep
-    // few threads of a CTA busy, so they get 64-thread CTAs: more of them fit an
-    // SM, and the groups take fewer waves
-    const int threads = B <= 2 ? 64 : NT;
-    group_gather_kernel<<<std::max(fe.ngroup_h, 1), threads, sizeof(double) * (size_t)cap, s>>>(fe, x, B, cap);
+    // the hanging groups; block 0 also writes the zero row.  (64-thread CTAs
+    // for narrow blocks were measured slower at c1: B = 1 HX 0.186 vs 0.169 ms)
+    group_gather_kernel<<<std::max(fe.ngroup_h, 1), NT, sizeof(double) * (size_t)cap, s>>>(fe, x, B, cap);
     INVDFT_LAUNCH_CHECK();
   }
 }
@@ -2524,7 +2541,7 @@ int launch_hx_assemble(const FeView &fe, const double *Ycell, double *out, int B
       INVDFT_CUDA(cudaFuncSetAttribute(group_partial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
       attr = true;
     }
-    group_partial_kernel<<<fe.ngroup_h, B <= 2 ? 64 : NT, sizeof(double) * (size_t)cap, s>>>(fe, Ycell, B, cap);
+    group_partial_kernel<<<fe.ngroup_h, NT, sizeof(double) * (size_t)cap, s>>>(fe, Ycell, B, cap);
     INVDFT_LAUNCH_CHECK();
     master_sum_kernel<<<ceil_div((int64_t)fe.nmast * B, NT), NT, 0, s>>>(fe, B, const_cast<double *>(Ycell));
     INVDFT_LAUNCH_CHECK();

@@ -442,7 +442,6 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
     n_masters = G.nmast;
     d_mslot.upload(mslot_h, s);
     d_g_rptr.upload(G.rptr, s);
-    d_g_rows.upload(G.rows.empty() ? std::vector<int>{0} : G.rows, s);
     d_g_hrow.upload(G.hrow.empty() ? std::vector<int>{0} : G.hrow, s);
     d_g_m0.upload(G.m0.empty() ? std::vector<int>{0} : G.m0, s);
     d_g_nm.upload(G.nm.empty() ? std::vector<int>{0} : G.nm, s);
@@ -534,13 +533,13 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   ldh = nd + (nd & 1);
   fe.n1 = n1; fe.nd = nd; fe.nq = nq; fe.nc = nc; fe.nnodes = nn; fe.ldh = ldh;
   fe.phi = phi.p; fe.cell_h = cell_h.p; fe.cell_nodes = cell_nodes.p; fe.cell_map = cell_map.p;
-  fe.cons_ptr = cpsi.ptr.p; fe.cons_masters = cpsi.masters.p; fe.cons_w = cpsi.w.p; fe.cons_gw = cons_gw.p;
-  fe.cons_rows = cpsi.rows.p; fe.ncons = cpsi.n;
+  fe.cons_ptr = cpsi.ptr.p; fe.cons_masters = cpsi.masters.p; fe.cons_gw = cons_gw.p;
+  fe.ncons = cpsi.n;
   fe.slot_of = d_slot_of.p; fe.dptr = d_dptr.p;
   fe.cell_map_t = cell_map_t.p; fe.slot_of_t = d_slot_of_t.p;
   fe.zptr = d_zptr.p; fe.nhang = nhang;
   fe.nmast = n_masters; fe.mslot = d_mslot.p;
-  fe.g_rptr = d_g_rptr.p; fe.g_rows = d_g_rows.p; fe.g_hrow = d_g_hrow.p; fe.g_m0 = d_g_m0.p;
+  fe.g_rptr = d_g_rptr.p; fe.g_hrow = d_g_hrow.p; fe.g_m0 = d_g_m0.p;
   fe.g_nm = d_g_nm.p; fe.g_poff = d_g_poff.p; fe.mp_ptr = d_mp_ptr.p; fe.mp_idx = d_mp_idx.p;
   fe.gpart = d_gpart.p;
   fe.g_woff = d_g_woff.p; fe.g_w = d_g_w.p; fe.g_wt = d_g_wt.p;

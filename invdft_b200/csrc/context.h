@@ -70,7 +70,7 @@ class Context {
   int64_t n_slots = 0;             // result slots of a cell product (per column)
   int n_masters = 0;
   // constraint groups (rows with identical master lists) and master pair lists
-  DevBuf<int> d_g_rptr, d_g_rows, d_g_hrow, d_g_m0, d_g_nm, d_g_poff, d_mp_ptr, d_mp_idx;
+  DevBuf<int> d_g_rptr, d_g_hrow, d_g_m0, d_g_nm, d_g_poff, d_mp_ptr, d_mp_idx;
   DevBuf<double> d_gpart;          // [npairs][64] per-(group, master) partial sums
   DevBuf<int64_t> d_g_woff;        // per-group start of its weight block
   DevBuf<double> d_g_w, d_g_wt;    // distinct group weight blocks, [row][master] and [master][row]

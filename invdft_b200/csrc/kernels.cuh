@@ -15,9 +15,7 @@ struct FeView {
   const int *cell_map;      // [nc*nd]: node (free) or -(1+constraint row)
   const int *cons_ptr;      // [ncons+1]
   const int *cons_masters;
-  const double *cons_w;     // plain weights
   const double *cons_gw;    // weights * M^-1/2[master] (Lowdin gather)
-  const int *cons_rows;     // [ncons]
   int ncons;
   // slot layout of cell results: row (cell, local) of a cell product is written
   // to slot slot_of[cell*nd+local] (-1: Dirichlet row, dropped).  Free nodes own
@@ -39,14 +37,14 @@ struct FeView {
   int nmast;
   const int *mslot;         // [nmast] the last slot of each master's range: its summed hanging contributions
   // constraint rows grouped by identical (ordered) master lists: group g owns
-  // rows g_rows[g_rptr[g] .. g_rptr[g+1]) (hanging indices g_hrow, -1 for
-  // Dirichlet rows), whose masters are cons_masters[g_m0[g] ..][0, g_nm[g]);
-  // groups [0, ngroup_h) have masters, the rest are Dirichlet rows.  Pair
-  // (g, t) of a hanging group is partial row g_poff[g] + t; master i sums the
-  // partial rows mp_idx[mp_ptr[i] .. mp_ptr[i+1]).
+  // the rows g_rptr[g] .. g_rptr[g+1] of the group order, whose hanging indices
+  // g_hrow are consecutive (-1 for Dirichlet rows) and whose masters are
+  // cons_masters[g_m0[g] ..][0, g_nm[g]); groups [0, ngroup_h) have masters,
+  // the rest are Dirichlet rows.  Pair (g, t) of a hanging group is partial
+  // row g_poff[g] + t; master i sums the partial rows mp_idx[mp_ptr[i] .. mp_ptr[i+1]).
   int ngroup, ngroup_h, g_maxnm, g_maxnr;
   int g_stage;              // shared staging per group, doubles; larger groups read global memory
-  const int *g_rptr, *g_rows, *g_hrow, *g_m0, *g_nm, *g_poff;
+  const int *g_rptr, *g_hrow, *g_m0, *g_nm, *g_poff;
   // the plain weights of group g's rows from g_woff[g]: [row q][master t]
   // (g_w, for the transpose) and [t][q] (g_wt, for the gather); groups with
   // identical weight blocks share one copy

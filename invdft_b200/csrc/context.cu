@@ -560,6 +560,10 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
     // INVDFT_MINRES_FUSED=0: the MINRES update as separate launches
     const char *mf = std::getenv("INVDFT_MINRES_FUSED");
     minres_fused = !(mf && std::string(mf) == "0");
+    // INVDFT_MINRES_GRAPH=1: each 8-iteration segment of the fused MINRES loop
+    // is captured once as a CUDA graph (per width and buffer set) and replayed
+    const char *mg = std::getenv("INVDFT_MINRES_GRAPH");
+    minres_graph = mg && std::string(mg) == "1";
     // INVDFT_TRACE=1: one line per Chebyshev pass on stderr (diagnostics)
     const char *tr = std::getenv("INVDFT_TRACE");
     trace = tr && std::string(tr) == "1";
@@ -586,7 +590,13 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   INVDFT_CUDA(cudaStreamSynchronize(s));
 }
 
+void Context::release_graphs() {
+  for (auto &g : seg_graphs) cudaGraphExecDestroy(g.exec);
+  seg_graphs.clear();
+}
+
 Context::~Context() {
+  release_graphs();
   for (auto e : ev_pool) cudaEventDestroy(e);
   if (stream) {
     cudaStreamSynchronize(stream);
@@ -705,7 +715,7 @@ int Context::sf_shape(const double *d_x, int Bw) {
 
 void Context::cell_gemm(const double *d_x, int Bw, bool low) {
   const int shape = (!low && hx_variant == 3) ? sf_shape(d_x, Bw) : 0;   // tuning stays outside the timing
-  const bool rec = profile && ev_used + 2 <= (int)ev_pool.size();
+  const bool rec = profile && !capturing && ev_used + 2 <= (int)ev_pool.size();
   if (rec) INVDFT_CUDA(cudaEventRecord(ev_pool[ev_used], stream));
   if (low && hx_variant == 3 && in_filter && ladder_operands == 1)
     launch_hx_cell_sf_tc(fe, sfm_tf32, vj.p, d_x, Ycell.p, Bw, GATHER_LOWDIN, stream);
@@ -1421,6 +1431,88 @@ void Context::minres_core(const double *d_rhs, double *d_x, double tol, int maxi
     m_ticket.alloc(2);
     m_ticket.zero(stream);
   }
+  // one iteration's launches (fused form: the HX chain with the MINRES
+  // epilogue, then the two fused updates; the host rotates the buffers)
+  auto rotate = [&]() {
+    // (r1, r2, yn) <- (r2, yn, r1): the new r2 was written over yn, r1 is free;
+    // the new w was written over w2
+    m_r1.swap(m_r2);
+    m_r2.swap(m_yn);
+    m_w.swap(m_w2);
+  };
+  auto iterate = [&](int itn) {
+    cell_gemm(m_v.p, Bc, low && hx_variant == 3);
+    AsmEpilogue epi;
+    epi.kind = AsmEpilogue::MINRES;
+    epi.in = m_v.p;
+    epi.prev = m_r1.p;
+    epi.eps = eps_c.p;
+    epi.minres_coef = st.coef1;
+    epi.dot_partial = partial.p;
+    if (minres_fused) {   // alpha reduced by the assembly's last CTA
+      epi.dot_out = st.alfa;
+      epi.dot_ticket = m_ticket.p + 1;
+    }
+    const int nparts = launch_hx_assemble(fe, Ycell.p, m_yn.p, Bc, epi, nblocks_red, stream);
+    if (nparts > 0) launch_reduce_partials(partial.p, nparts, Bc, st.alfa, stream);
+    if (minres_fused) {
+      launch_minres_update1_fused(m_r2.p, m_yn.p, m_y.p, diagA.p, st, nn, Bc, partial.p, nblocks_red,
+                                  m_ticket.p, stream);
+      launch_minres_update2v(m_xc.p, m_w.p, m_w2.p, m_v.p, m_y.p, st, nn, Bc, stream);
+      rotate();
+    } else {
+      launch_minres_update1(m_r1.p, m_r2.p, m_y.p, m_yn.p, diagA.p, st, nn, Bc, partial.p, nblocks_red, stream);
+      launch_minres_scalars(st, Bc, itn, stream);
+      launch_minres_update2(m_xc.p, m_w.p, m_w2.p, m_v.p, st, nn, Bc, stream);
+      need_v = true;
+    }
+  };
+  // len fused iterations from a CUDA graph, captured on the first use of this
+  // width, tolerance and buffer set; a replay leaves the host's buffer
+  // rotation where the captured iterations left it
+  auto graph_segment = [&](int len) {
+    uint64_t tolbits;
+    std::memcpy(&tolbits, &st.tol, sizeof(tolbits));
+    const std::vector<uintptr_t> key = {
+        (uintptr_t)Bc, (uintptr_t)len, (uintptr_t)(low ? 1 : 0), (uintptr_t)tolbits,
+        (uintptr_t)(hx_variant == 3 ? sf_tuned[std::min(Bc, 64)] : -1),
+        (uintptr_t)m_v.p, (uintptr_t)m_yn.p, (uintptr_t)m_r1.p, (uintptr_t)m_r2.p, (uintptr_t)m_y.p,
+        (uintptr_t)m_w.p, (uintptr_t)m_w2.p, (uintptr_t)m_xc.p, (uintptr_t)eps_c.p, (uintptr_t)partial.p,
+        (uintptr_t)m_scal.p, (uintptr_t)m_flags.p, (uintptr_t)m_ticket.p, (uintptr_t)Ycell.p,
+        (uintptr_t)diagA.p, (uintptr_t)vj.p};
+    for (auto &g : seg_graphs)
+      if (g.key == key) {
+        INVDFT_CUDA(cudaGraphLaunch(g.exec, stream));
+        count_launches(g.launches);
+        for (int k = 0; k < len; ++k) rotate();
+        return;
+      }
+    if (seg_graphs.size() >= 48) release_graphs();
+    const long long l0 = launch_count();
+    INVDFT_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    capturing = true;
+    cudaGraph_t graph = nullptr;
+    try {
+      for (int k = 0; k < len; ++k) iterate(0);
+    } catch (...) {
+      capturing = false;
+      cudaStreamEndCapture(stream, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      (void)cudaGetLastError();
+      throw;
+    }
+    capturing = false;
+    INVDFT_CUDA(cudaStreamEndCapture(stream, &graph));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      throw StatusError(INVDFT_CUDA_ERROR, std::string("CUDA graph instantiation: ") + cudaGetErrorString(e));
+    }
+    INVDFT_CUDA(cudaGraphLaunch(exec, stream));   // the capture moved the rotation already
+    seg_graphs.push_back({key, exec, launch_count() - l0});
+  };
   for (int itn = 1; itn <= maxit; ++itn) {
     if ((itn - 1) % check_every == 0) {
       if (trace) INVDFT_CUDA(cudaEventRecord(seg_ev[1], stream));
@@ -1446,37 +1538,22 @@ void Context::minres_core(const double *d_rhs, double *d_x, double tol, int maxi
     }
     if (need_v) launch_minres_v(m_y.p, st, m_v.p, nn, Bc, stream);   // else left by the fused update2
     need_v = false;
-    cell_gemm(m_v.p, Bc, low && hx_variant == 3);
-    AsmEpilogue epi;
-    epi.kind = AsmEpilogue::MINRES;
-    epi.in = m_v.p;
-    epi.prev = m_r1.p;
-    epi.eps = eps_c.p;
-    epi.minres_coef = st.coef1;
-    epi.dot_partial = partial.p;
-    if (minres_fused) {   // alpha reduced by the assembly's last CTA
-      epi.dot_out = st.alfa;
-      epi.dot_ticket = m_ticket.p + 1;
+    if (minres_graph && minres_fused && itn > check_every && (itn - 1) % check_every == 0 &&
+        itn + check_every - 1 <= maxit) {
+      // the whole segment from a CUDA graph: the first segment of the solve ran
+      // as plain launches, so every kernel and this width's launch shape are set up
+      if (hx_variant == 3 && !low) (void)sf_shape(m_v.p, Bc);
+      graph_segment(check_every);
+      n_hx += check_every;
+      n_hx_cols += (int64_t)Bc * check_every;
+      width_iters[Bc] += check_every;
+      itn += check_every - 1;
+      continue;
     }
-    const int nparts = launch_hx_assemble(fe, Ycell.p, m_yn.p, Bc, epi, nblocks_red, stream);
-    if (nparts > 0) launch_reduce_partials(partial.p, nparts, Bc, st.alfa, stream);
+    iterate(itn);
     n_hx++;
     n_hx_cols += Bc;
     width_iters[Bc]++;
-    if (minres_fused) {
-      launch_minres_update1_fused(m_r2.p, m_yn.p, m_y.p, diagA.p, st, nn, Bc, partial.p, nblocks_red,
-                                  m_ticket.p, stream);
-      // (r1, r2, yn) <- (r2, yn, r1): the new r2 was written over yn, r1 is free
-      m_r1.swap(m_r2);
-      m_r2.swap(m_yn);
-      launch_minres_update2v(m_xc.p, m_w.p, m_w2.p, m_v.p, m_y.p, st, nn, Bc, stream);
-      m_w.swap(m_w2);   // the new w was written over w2
-    } else {
-      launch_minres_update1(m_r1.p, m_r2.p, m_y.p, m_yn.p, diagA.p, st, nn, Bc, partial.p, nblocks_red, stream);
-      launch_minres_scalars(st, Bc, itn, stream);
-      launch_minres_update2(m_xc.p, m_w.p, m_w2.p, m_v.p, st, nn, Bc, stream);
-      need_v = true;
-    }
   }
   scatter_x();
   std::vector<int> it_now(Bc);

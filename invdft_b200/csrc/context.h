@@ -56,6 +56,15 @@ class Context {
   int hx_variant = 3;
   int sf_tune = -1;                // launch shape of the matrix-free kernel (-1: autotuned per width)
   bool minres_fused = true;        // MINRES update1 + reductions + scalars, update2 + v, in two launches
+  bool minres_graph = false;       // INVDFT_MINRES_GRAPH=1: fused MINRES segments replayed from CUDA graphs
+  bool capturing = false;          // a CUDA graph capture is in progress (no profiling events)
+  struct SegGraph {                // one captured MINRES segment
+    std::vector<uintptr_t> key;    // width, precision, tolerance bits and every buffer it touches
+    cudaGraphExec_t exec;
+    long long launches;            // kernels per replay
+  };
+  std::vector<SegGraph> seg_graphs;
+  void release_graphs();
   bool trace = false;              // per-pass lines of the eigensolver on stderr
   int sf_tuned[65];                // autotuned shape per block width (-1: not measured yet)
   int sf_shape(const double *d_x, int Bw);

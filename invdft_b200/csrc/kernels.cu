@@ -2061,6 +2061,7 @@ std::atomic<long long> g_launches{0};
 
 long long launch_count() { return g_launches.load(); }
 void count_launch() { g_launches.fetch_add(1); }
+void count_launches(long long n) { g_launches.fetch_add(n); }
 
 // ---------------------------------------------------------------------------
 // launch wrappers (each counts its launches)

@@ -66,6 +66,7 @@ enum GatherMode { GATHER_LOWDIN = 0, GATHER_PLAIN = 1 };
 // ---- launches (implemented in kernels.cu) ----
 long long launch_count();  // kernels launched by this library so far
 void count_launch();       // for launches made outside kernels.cu
+void count_launches(long long n);   // the kernels of a replayed CUDA graph
 void launch_build_cell_h(const FeView &fe, const double *vks, const double *jxw, const double *Kref,
                          double *H, cudaStream_t s);
 void launch_hx_cell_gemm(const FeView &fe, const double *H, const double *x, double *Ycell, int B,

@@ -590,7 +590,11 @@ Context::Context(const invdft_problem_desc *d, const invdft_params *pp) {
   INVDFT_CUDA(cudaStreamSynchronize(s));
 }
 
+// Destroys the cached MINRES segment graphs, after the stream has finished
+// any replay of them.
 void Context::release_graphs() {
+  if (seg_graphs.empty()) return;
+  if (stream) cudaStreamSynchronize(stream);
   for (auto &g : seg_graphs) cudaGraphExecDestroy(g.exec);
   seg_graphs.clear();
 }

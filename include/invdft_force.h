@@ -388,7 +388,7 @@ invdft_status invdft_bfgs_run(invdft_ctx *ctx, double *pot, const invdft_bfgs_op
  * lazily: the first call on a device loads the module, which reserves the
  * array and the kernels' own device memory, so a caller that owns its device
  * pool makes one warm-up call on each device before handing the device to its
- * pool or starting a stream capture; later calls allocate nothing.  Every call
+ * pool; later calls allocate nothing.  Every call
  * looks up the array's device address with the device current (no allocation
  * once the module is loaded), so the address stays right after a device reset.
  * Calls share the array: calls that overlap on the GPU race.  Asynchronous

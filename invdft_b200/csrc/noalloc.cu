@@ -18,7 +18,7 @@
 // The module is loaded lazily: the first call on a device loads it, which is
 // when the array and the kernels' own device memory are reserved.  A caller
 // that owns its device pool makes one warm-up call per device before it hands
-// the device to the pool or starts a stream capture.  The array's name in host
+// the device to the pool.  The array's name in host
 // code is a host-side stand-in, not a device address, so every call asks the
 // runtime for the address with the device current; once the module is loaded
 // the lookup allocates nothing, and it stays right when a device reset or a

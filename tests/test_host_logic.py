@@ -1,5 +1,6 @@
-"""Host-side logic on CPU: the L-BFGS mirror, block partitioning, and the
-replica aggregation of bench.py over two gloo ranks."""
+"""Host-side logic on CPU: the L-BFGS mirror, block partitioning, the
+replica aggregation of bench.py over two gloo ranks, and bench.py's reference
+arm."""
 import os
 import sys
 
@@ -99,3 +100,27 @@ def test_bench_workload_names_and_profile_traffic():
     assert bench.workload_name("c0_lih", P, "fp64").startswith("c0_lih: LiH-like")
     cap = bench._traffic_from_profiles("c1_c2h4:sf:fp64")
     assert cap["columns"] == 16 and cap["bytes"] > 0
+
+
+def test_reference_arm_runs_the_cpu_restatement_without_the_gpu_library():
+    """bench.py --impl reference: whole force evaluations of the C++
+    restatement on the host cores, one JSON line with the driver's keys, and
+    none of the product's CUDA code loaded in the process."""
+    import json
+    import subprocess
+    code = (
+        "import sys, json, runpy\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--config', 'tiny_h2', '--steps', '1', '--warmup', '1',"
+        " '--ref-budget-s', '5']\n"
+        "runpy.run_path('bench.py', run_name='__main__')\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print(json.dumps({'product_so_loaded': 'libinvdft_b200' in maps}))\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(l) for l in r.stdout.strip().splitlines() if l.startswith("{")]
+    line, probe = lines[-2], lines[-1]
+    assert line["impl"] == "reference" and line["value"] > 0 and line["steps"] >= 1
+    assert line["unit"] == "force-evals/s" and line["higher_is_better"] is True
+    assert line["cpu_baseline"]["kind"] in ("port", "reference") and line["cpu_baseline"]["value"] == line["value"]
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert not probe["product_so_loaded"]

@@ -19,17 +19,20 @@ struct FeView {
   int ncons;
   // slot layout of cell results: row (cell, local) of a cell product is written
   // to slot slot_of[cell*nd+local] (-1: Dirichlet row, dropped).  Free nodes own
-  // the contiguous slots [dptr[n], dptr[n+1]); rows of hanging nodes live in
-  // slots after those, are summed per hanging node into z and reach their
-  // masters through the constraint groups below.
+  // the contiguous slots [dptr[n], dptr[n+1]), a master of hanging nodes one
+  // more (the last, for its hanging contributions); rows of hanging nodes live
+  // in slots after those, contiguous per hanging node in hanging-index order,
+  // and reach their masters through the constraint groups below.
   const int *slot_of;       // [nc*nd]
-  // the Lowdin gather map and the slot map transposed, [nd][nc]: for blocks
-  // narrower than 16 columns a CTA of the matrix-free kernel holds several
-  // cells, whose entries for one local index are then contiguous
+  // the matrix-free kernel's gather map (cell_map_sf) and the slot map
+  // transposed, [nd][nc]: for blocks narrower than 16 columns a CTA of the
+  // matrix-free kernel holds several cells, whose entries for one local index
+  // are then contiguous
   const int *cell_map_t;
   const int *slot_of_t;
   // the matrix-free kernel's row-major gather map: node, or -(1 + row of hvg)
-  // for a constrained entry (cell_map_t is its transpose)
+  // for a constrained entry (the hanging index, or nhang for the zero row of
+  // the Dirichlet entries)
   const int *cell_map_sf;
   const int *dptr;          // [nnodes+1]
   const int *zptr;          // [nhang+1] slot ranges of the hanging nodes' rows
